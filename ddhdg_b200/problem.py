@@ -308,7 +308,9 @@ class NPSolverParameters:
                  nonlinear_parameters: NonlinearSolverParameters = None,
                  iterative_linear_solver: bool = False, multithreading: bool = True,
                  dd_flux_type: DDFluxType = DDFluxType.use_cell,
-                 phi_linearize: bool = False, precision: Precision = Precision.fp64):
+                 phi_linearize: bool = False, precision: Precision = Precision.fp64,
+                 consistent_drift_jacobian: bool = False,
+                 consistent_recombination_jacobian: bool = False):
         if not (V_degree == n_degree == p_degree):
             raise NotImplementedError("V, n and p must share one polynomial degree")
         self.degree = {Component.V: int(V_degree), Component.n: int(n_degree),
@@ -319,6 +321,15 @@ class NPSolverParameters:
         self.dd_flux_type = DDFluxType(dd_flux_type)
         self.phi_linearize = bool(phi_linearize)
         self.precision = Precision(precision)
+        # Off by default: the reference's Jacobian.  Its cell drift term
+        # couples E with the sign opposite to the residual's derivative
+        # (include/assembling_methods.template.h:500 and :522 against the
+        # residual at :656 and :673) and its recombination derivatives miss
+        # the doping magnitude (src/recombination_term.cpp:473-475 with
+        # src/adimensionalizer.cpp:476-497).  Both options only change the
+        # Jacobian, never the residual, so converged solutions are the same.
+        self.consistent_drift_jacobian = bool(consistent_drift_jacobian)
+        self.consistent_recombination_jacobian = bool(consistent_recombination_jacobian)
 
     @property
     def k(self) -> int:
@@ -335,10 +346,13 @@ class FixedTauNPSolverParameters(NPSolverParameters):
                  V_tau: float = 1.0, n_tau: float = 1.0, p_tau: float = 1.0,
                  iterative_linear_solver: bool = False, multithreading: bool = True,
                  dd_flux_type: DDFluxType = DDFluxType.use_cell,
-                 phi_linearize: bool = False, precision: Precision = Precision.fp64):
+                 phi_linearize: bool = False, precision: Precision = Precision.fp64,
+                 consistent_drift_jacobian: bool = False,
+                 consistent_recombination_jacobian: bool = False):
         super().__init__(V_degree, n_degree, p_degree, nonlinear_parameters,
                          iterative_linear_solver, multithreading, dd_flux_type,
-                         phi_linearize, precision)
+                         phi_linearize, precision, consistent_drift_jacobian,
+                         consistent_recombination_jacobian)
         self.tau = {Component.V: float(V_tau), Component.n: float(n_tau),
                     Component.p: float(p_tau)}
 

@@ -83,6 +83,10 @@ extern "C"
     const double *tau;                   // [ncells*2*dim*3] rescaled tau
     const int    *face_bc;               // [nfaces*3]: 0 none, 1 Dirichlet, 2 Neumann
     const double *face_bc_val;           // [nfaces*3*nqf] already rescaled
+    // Jacobian options; 0 reproduces the reference exactly.
+    //  bit 0: consistent sign of the E coupling of the cell drift terms
+    //  bit 1: recombination derivatives scaled by the doping magnitude
+    int jacobian_fix;
   };
 }
 
@@ -804,6 +808,12 @@ namespace
       r /= P.rec_rescale;
       drn /= P.rec_rescale;
       drp /= P.rec_rescale;
+      if (P.jacobian_fix & 2)
+        {
+          // d(R/R_s)/d(n/N) = N dR/dn / R_s; the reference omits the N
+          drn *= rf;
+          drp *= rf;
+        }
     }
 
     double
@@ -841,6 +851,7 @@ namespace
 
       const double U_T = (KB * P.temperature / Q) / P.thermal_voltage_rescale;
       const double eps = P.eps, mun = P.mu_n, mup = P.mu_p;
+      const double drift_sign = (P.jacobian_fix & 1) ? -1. : 1.;
 
       // ---- prepare_data_on_cell_quadrature_points (T:134-265)
       std::vector<double> V0(nqc), n0(nqc), p0(nqc), rr(nqc, 0.), drn(nqc, 0.),
@@ -930,9 +941,11 @@ namespace
                   {
                     const Vec mun_E   = scale(dd[0][j], mun);
                     const Vec Dn_Wn   = scale(scale(dd[1][j], mun), U_T);
+                    // the reference adds +n0 (mu E_j . grad z) here although
+                    // the residual's derivative is -n0 (mu dE . grad z)
                     s += (-cvv[1][j] * ddiv[1][i] + dot(dd[1][j], dd[1][i], dim) -
                           cvv[1][j] * dot(mun_E0, cg[1][i], dim) +
-                          n0[q] * dot(mun_E, cg[1][i], dim) +
+                          drift_sign * n0[q] * dot(mun_E, cg[1][i], dim) +
                           dot(Dn_Wn, cg[1][i], dim) -
                           (drn[q] * cvv[1][j] + drp[q] * cvv[2][j]) * cvv[1][i]) *
                          JxW;
@@ -943,7 +956,7 @@ namespace
                     const Vec Dp_Wp = scale(scale(dd[2][j], mup), U_T);
                     s += (-cvv[2][j] * ddiv[2][i] + dot(dd[2][j], dd[2][i], dim) +
                           cvv[2][j] * dot(mup_E0, cg[2][i], dim) -
-                          p0[q] * dot(mup_E, cg[2][i], dim) +
+                          drift_sign * p0[q] * dot(mup_E, cg[2][i], dim) +
                           dot(Dp_Wp, cg[2][i], dim) -
                           (drn[q] * cvv[1][j] + drp[q] * cvv[2][j]) * cvv[2][i]) *
                          JxW;

@@ -87,6 +87,7 @@ class OrProblem(ctypes.Structure):
         ("rec_c", ctypes.POINTER(ctypes.c_double)),
         ("doping", ctypes.POINTER(ctypes.c_double)), ("tau", ctypes.POINTER(ctypes.c_double)),
         ("face_bc", ctypes.POINTER(ctypes.c_int)), ("face_bc_val", ctypes.POINTER(ctypes.c_double)),
+        ("jacobian_fix", ctypes.c_int),
     ]
 
 
@@ -270,6 +271,8 @@ class OracleSolver:
             P.enabled[c] = int(en[c])
         P.flux = int(prm.dd_flux_type)
         P.phi_linearize = int(prm.phi_linearize)
+        P.jacobian_fix = (1 if getattr(prm, "consistent_drift_jacobian", False) else 0) | \
+            (2 if getattr(prm, "consistent_recombination_jacobian", False) else 0)
         if probe:
             return P
         r = self._rescale()
