@@ -1,0 +1,1342 @@
+// C ABI of the B200 HDG hot path: context set-up (NPSolver construction and
+// setup_overall_system, src/np_solver.cpp:553-655), the per-cell
+// condensation and reconstruction launches, the global trace assembly
+// (copy_local_to_global, src/np_solver.cpp:1293-1322), the global trace
+// solve (solve_linear_problem, src/np_solver.cpp:1326-1354) and the Newton
+// loop (private_run, src/np_solver.cpp:1452-1561).
+#include <cuda_runtime.h>
+#include <cusolverSp.h>
+#include <cusparse.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/ddhdg_b200.h"
+#include "hdg_kernels.cuh"
+#include "hdg_tables.h"
+
+using namespace ddhdg;
+
+namespace
+{
+  thread_local std::string g_last_error;
+
+  int
+  fail(int code, const std::string &msg)
+  {
+    g_last_error = msg;
+    return code;
+  }
+
+#define CK(call)                                                              \
+  do                                                                          \
+    {                                                                         \
+      cudaError_t e_ = (call);                                                \
+      if (e_ != cudaSuccess)                                                  \
+        return fail(DDHDG_CUDA_ERROR, std::string(#call) + ": " +             \
+                                        cudaGetErrorString(e_));              \
+    }                                                                         \
+  while (0)
+
+  template <typename T>
+  struct DevBuf
+  {
+    T     *p = nullptr;
+    size_t n = 0;
+    int
+    alloc(size_t count)
+    {
+      if (count <= n && p)
+        return DDHDG_OK;
+      if (p)
+        cudaFree(p);
+      p = nullptr;
+      n = 0;
+      if (count == 0)
+        return DDHDG_OK;
+      if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess)
+        {
+          cudaGetLastError();
+          return fail(DDHDG_OOM, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
+        }
+      n = count;
+      return DDHDG_OK;
+    }
+    int
+    upload(const T *h, size_t count)
+    {
+      int r = alloc(count);
+      if (r)
+        return r;
+      if (count && cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(DDHDG_CUDA_ERROR, "upload failed");
+      return DDHDG_OK;
+    }
+    void
+    release()
+    {
+      if (p)
+        cudaFree(p);
+      p = nullptr;
+      n = 0;
+    }
+    ~DevBuf() { release(); }
+  };
+
+  // per mode (0: regular run, 1: thermodynamic equilibrium = V only)
+  struct Mode
+  {
+    int                   comps[3] = {0, 1, 2};
+    int                   ncomp    = 0;
+    int                   Nt       = 0;
+    int                   ncol     = 0;
+    int                   ycols    = 0;
+    int64_t               ndofs    = 0;
+    int64_t               nnz      = 0;
+    DevBuf<int32_t>       rowptr, colind;
+    DevBuf<uint8_t>       slots; // [ncells][F][F]
+    DevBuf<double>        ycache, tt, rhs, dval, csr, grhs, x, dtrace, dcell;
+    DevBuf<int32_t>       dflag;
+    std::vector<int32_t>  perm; // nested-dissection order of the trace dofs
+    DevBuf<int32_t>       d_perm, d_iperm, prow, pcol;
+    DevBuf<int32_t>       pmap; // permuted position of each CSR entry
+    DevBuf<double>        pval, pb, px;
+    bool                  built = false;
+  };
+} // namespace
+
+struct ddhdg_ctx
+{
+  ddhdg_problem_desc desc{};
+  int                dim = 0, k = 0, nb = 0, nf = 0, nqc = 0, nqf = 0, F = 0;
+  int64_t            ncells = 0, nfaces = 0;
+  int64_t            face_off[3]    = {0, 0, 0};
+  int                face_ext[3][3] = {{1, 1, 1}, {1, 1, 1}, {1, 1, 1}};
+  int                enabled[3]     = {1, 1, 1};
+  Tables             T;
+  TabOff             to{};
+  DevBuf<double>     tables, doping, rec_a, rec_b, rec_c, tau_table, bc_val;
+  DevBuf<int32_t>    bc;
+  DevBuf<int>        status;
+  Mode               mode[2];
+  int                sm_count = 148;
+  cusolverSpHandle_t sp       = nullptr;
+  cusparseMatDescr_t descr    = nullptr;
+  // face -> adjacent cells
+  std::vector<int64_t> face_cells; // [nfaces][2] (-1 when absent)
+  double             t_condense = 0., t_solve = 0., t_recon = 0.;
+  int                t_steps    = 0;
+  DevBuf<double>     norm_buf;
+  DevBuf<int64_t>    d_face_cells, d_face_local;
+};
+
+namespace
+{
+  int
+  ncol_for(const ddhdg_ctx *c, const Mode &m)
+  {
+    return (c->desc.flux == DDHDG_FLUX_USE_CELL) ? 1 + m.Nt : 1 + 2 * m.Nt;
+  }
+
+  void
+  set_mode_comps(ddhdg_ctx *c, int thermo)
+  {
+    Mode &m = c->mode[thermo];
+    m.ncomp = 0;
+    if (thermo)
+      m.comps[m.ncomp++] = 0;
+    else
+      for (int b = 0; b < 3; ++b)
+        if (c->enabled[b])
+          m.comps[m.ncomp++] = b;
+    m.Nt    = c->F * m.ncomp * c->nf;
+    m.ncol  = ncol_for(c, m);
+    m.ycols = 1 + m.Nt;
+    m.ndofs = c->nfaces * m.ncomp * c->nf;
+  }
+
+  int64_t
+  face_of_cell(const ddhdg_ctx *c, int64_t cell, int f)
+  {
+    int ci[3];
+    ci[0] = (int)(cell % c->desc.n[0]);
+    ci[1] = (int)((cell / c->desc.n[0]) % (c->dim > 1 ? c->desc.n[1] : 1));
+    ci[2] = (int)(cell / ((int64_t)c->desc.n[0] * (c->dim > 1 ? c->desc.n[1] : 1)));
+    const int a = f / 2;
+    ci[a] += f % 2;
+    int64_t idx = 0, stride = 1;
+    for (int b = 0; b < c->dim; ++b)
+      {
+        idx += ci[b] * stride;
+        stride *= c->face_ext[a][b];
+      }
+    return c->face_off[a] + idx;
+  }
+
+  // Nested-dissection order of the faces of the structured mesh: recursive
+  // bisection of the cell box along its longest axis; the faces of the
+  // separating plane are numbered after both halves.
+  void
+  nd_order(const ddhdg_ctx *c, std::vector<int64_t> &order)
+  {
+    std::vector<char> used(c->nfaces, 0);
+    order.clear();
+    order.reserve(c->nfaces);
+    struct Box
+    {
+      int lo[3], hi[3];
+    };
+    // faces of a box: all faces of its cells not yet numbered
+    std::function<void(Box)> rec = [&](Box b) {
+      int ext[3], ax = 0, best = 0;
+      int64_t ncell = 1;
+      for (int a = 0; a < 3; ++a)
+        {
+          ext[a] = b.hi[a] - b.lo[a];
+          ncell *= ext[a];
+          if (a < c->dim && ext[a] > best)
+            {
+              best = ext[a];
+              ax   = a;
+            }
+        }
+      if (ncell <= 4 || best <= 1)
+        {
+          for (int z = b.lo[2]; z < b.hi[2]; ++z)
+            for (int y = b.lo[1]; y < b.hi[1]; ++y)
+              for (int x = b.lo[0]; x < b.hi[0]; ++x)
+                {
+                  const int64_t cell =
+                    x + (int64_t)c->desc.n[0] * (y + (int64_t)(c->dim > 1 ? c->desc.n[1] : 1) * z);
+                  for (int f = 0; f < c->F; ++f)
+                    {
+                      const int64_t Fi = face_of_cell(c, cell, f);
+                      if (!used[Fi])
+                        {
+                          used[Fi] = 1;
+                          order.push_back(Fi);
+                        }
+                    }
+                }
+          return;
+        }
+      const int mid = b.lo[ax] + ext[ax] / 2;
+      // separator: faces with normal ax at position mid inside the box
+      std::vector<int64_t> sep;
+      int                  lo[3] = {b.lo[0], b.lo[1], b.lo[2]};
+      int                  hi[3] = {b.hi[0], b.hi[1], b.hi[2]};
+      lo[ax] = mid;
+      hi[ax] = mid + 1;
+      for (int z = lo[2]; z < hi[2]; ++z)
+        for (int y = lo[1]; y < hi[1]; ++y)
+          for (int x = lo[0]; x < hi[0]; ++x)
+            {
+              const int64_t cell =
+                x + (int64_t)c->desc.n[0] * (y + (int64_t)(c->dim > 1 ? c->desc.n[1] : 1) * z);
+              const int64_t Fi = face_of_cell(c, cell, 2 * ax);
+              if (!used[Fi])
+                {
+                  used[Fi] = 1;
+                  sep.push_back(Fi);
+                }
+            }
+      Box b1 = b, b2 = b;
+      b1.hi[ax] = mid;
+      b2.lo[ax] = mid;
+      rec(b1);
+      rec(b2);
+      for (auto f : sep)
+        order.push_back(f);
+    };
+    Box all;
+    for (int a = 0; a < 3; ++a)
+      {
+        all.lo[a] = 0;
+        all.hi[a] = (a < c->dim) ? c->desc.n[a] : 1;
+      }
+    rec(all);
+  }
+
+  // Global trace sparsity (DoFTools::make_sparsity_pattern on the
+  // restricted trace dofs, src/np_solver.cpp:643-651) and the scatter slots.
+  int
+  build_mode(ddhdg_ctx *c, int thermo)
+  {
+    Mode &m = c->mode[thermo];
+    set_mode_comps(c, thermo);
+    const int     F = c->F, nf = c->nf, nc = m.ncomp;
+    const int64_t nfaces = c->nfaces;
+    // neighbour faces of every face
+    std::vector<std::vector<int64_t>> nbr(nfaces);
+    for (int64_t f = 0; f < nfaces; ++f)
+      for (int s = 0; s < 2; ++s)
+        {
+          const int64_t cell = c->face_cells[f * 2 + s];
+          if (cell < 0)
+            continue;
+          for (int g = 0; g < F; ++g)
+            nbr[f].push_back(face_of_cell(c, cell, g));
+        }
+    for (auto &v : nbr)
+      {
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+      }
+    const int64_t        ndofs = nfaces * nc * nf;
+    std::vector<int32_t> rowptr(ndofs + 1, 0);
+    int64_t              nnz = 0;
+    for (int64_t f = 0; f < nfaces; ++f)
+      for (int r = 0; r < nc * nf; ++r)
+        {
+          rowptr[f * nc * nf + r] = (int32_t)nnz;
+          nnz += (int64_t)nbr[f].size() * nc * nf;
+        }
+    rowptr[ndofs] = (int32_t)nnz;
+    if (nnz > INT32_MAX)
+      return fail(DDHDG_BAD_ARG, "global trace matrix too large for 32-bit CSR");
+    std::vector<int32_t> colind(nnz);
+    for (int64_t f = 0; f < nfaces; ++f)
+      for (int r = 0; r < nc * nf; ++r)
+        {
+          int64_t p = rowptr[f * nc * nf + r];
+          for (auto g : nbr[f])
+            for (int cc = 0; cc < nc * nf; ++cc)
+              colind[p++] = (int32_t)(g * nc * nf + cc);
+        }
+    std::vector<uint8_t> slots(c->ncells * F * F);
+    for (int64_t cell = 0; cell < c->ncells; ++cell)
+      for (int fi = 0; fi < F; ++fi)
+        {
+          const int64_t Fi = face_of_cell(c, cell, fi);
+          for (int fj = 0; fj < F; ++fj)
+            {
+              const int64_t Fj = face_of_cell(c, cell, fj);
+              const auto    it = std::lower_bound(nbr[Fi].begin(), nbr[Fi].end(), Fj);
+              slots[(cell * F + fi) * F + fj] = (uint8_t)(it - nbr[Fi].begin());
+            }
+        }
+    int r;
+    if ((r = m.rowptr.upload(rowptr.data(), rowptr.size())))
+      return r;
+    if ((r = m.colind.upload(colind.data(), colind.size())))
+      return r;
+    if ((r = m.slots.upload(slots.data(), slots.size())))
+      return r;
+    m.nnz = nnz;
+    // nested-dissection permutation of the dofs for the sparse QR solve
+    std::vector<int64_t> forder;
+    nd_order(c, forder);
+    std::vector<int32_t> perm(ndofs), iperm(ndofs);
+    int64_t              q = 0;
+    for (auto f : forder)
+      for (int cc = 0; cc < nc * nf; ++cc)
+        perm[q++] = (int32_t)(f * nc * nf + cc);
+    for (int64_t i = 0; i < ndofs; ++i)
+      iperm[perm[i]] = (int32_t)i;
+    // permuted matrix B = A(perm, perm): rows in new order, columns renumbered
+    std::vector<int32_t> prow(ndofs + 1, 0), pcol(nnz), pmap(nnz);
+    int64_t              pp = 0;
+    for (int64_t i = 0; i < ndofs; ++i)
+      {
+        prow[i]            = (int32_t)pp;
+        const int64_t  old = perm[i];
+        std::vector<std::pair<int32_t, int32_t>> ent;
+        for (int64_t e = rowptr[old]; e < rowptr[old + 1]; ++e)
+          ent.push_back({iperm[colind[e]], (int32_t)e});
+        std::sort(ent.begin(), ent.end());
+        for (auto &pr : ent)
+          {
+            pcol[pp] = pr.first;
+            pmap[pp] = pr.second;
+            ++pp;
+          }
+      }
+    prow[ndofs] = (int32_t)pp;
+    if ((r = m.d_perm.upload(perm.data(), perm.size())))
+      return r;
+    if ((r = m.d_iperm.upload(iperm.data(), iperm.size())))
+      return r;
+    if ((r = m.prow.upload(prow.data(), prow.size())))
+      return r;
+    if ((r = m.pcol.upload(pcol.data(), pcol.size())))
+      return r;
+    if ((r = m.pmap.upload(pmap.data(), pmap.size())))
+      return r;
+    m.built = true;
+    return DDHDG_OK;
+  }
+
+  int
+  ensure_buffers(ddhdg_ctx *c, int thermo)
+  {
+    Mode &m = c->mode[thermo];
+    int   r;
+    if (!m.built && (r = build_mode(c, thermo)))
+      return r;
+    const int64_t nc = c->ncells;
+    const int     Ns = m.ncomp * c->nb;
+    if ((r = m.ycache.alloc(nc * Ns * m.ycols)))
+      return r;
+    if ((r = m.tt.alloc(nc * m.Nt * m.Nt)))
+      return r;
+    if ((r = m.rhs.alloc(nc * m.Nt)))
+      return r;
+    if ((r = m.dval.alloc(nc * m.Nt)))
+      return r;
+    if ((r = m.dflag.alloc(nc * m.Nt)))
+      return r;
+    return DDHDG_OK;
+  }
+
+  KParams
+  make_params(ddhdg_ctx *c, int thermo)
+  {
+    Mode     &m = c->mode[thermo];
+    KParams   P{};
+    const auto &d = c->desc;
+    for (int a = 0; a < 3; ++a)
+      {
+        P.n[a]        = (a < c->dim) ? d.n[a] : 1;
+        P.face_off[a] = c->face_off[a];
+        for (int b = 0; b < 3; ++b)
+          P.face_ext[a][b] = c->face_ext[a][b];
+      }
+    P.ncells      = c->ncells;
+    P.tables      = c->tables.p;
+    P.to          = c->to;
+    P.eps         = d.eps;
+    P.mun         = d.mu_n;
+    P.mup         = d.mu_p;
+    P.U_T         = (KB_ * d.temperature / Q_) / d.thermal_voltage_rescale;
+    P.T           = d.temperature;
+    P.V_rescale   = d.V_rescale;
+    P.n_rescale   = d.n_rescale;
+    P.rec_rescale = d.rec_rescale;
+    P.nc          = d.nc;
+    P.nv          = d.nv;
+    P.ec          = d.ec_eV * EV_;
+    P.ev          = d.ev_eV * EV_;
+    P.rec_type    = d.rec_type;
+    P.srh_ni      = d.srh_ni;
+    P.srh_tau_n   = d.srh_tau_n;
+    P.srh_tau_p   = d.srh_tau_p;
+    P.rec_a       = c->rec_a.p;
+    P.rec_b       = c->rec_b.p;
+    P.rec_c       = c->rec_c.p;
+    P.doping      = c->doping.p;
+    P.tau_table   = c->tau_table.p;
+    for (int b = 0; b < 3; ++b)
+      P.tau[b] = d.tau[b];
+    P.face_bc     = c->bc.p;
+    P.face_bc_val = c->bc_val.p;
+    for (int b = 0; b < 3; ++b)
+      P.comps[b] = m.comps[b];
+    P.ncomp         = m.ncomp;
+    P.flux          = d.flux;
+    P.phi_linearize = d.phi_linearize;
+    P.thermo        = thermo;
+    P.jfix          = d.jacobian_fix;
+    P.ncol          = m.ncol;
+    P.ycols         = m.ycols;
+    P.status        = c->status.p;
+    return P;
+  }
+
+  using CondenseFn    = void (*)(KParams);
+  using ReconstructFn = void (*)(KParams, const double *, double *);
+
+  template <int D, int K>
+  void
+  pick(CondenseFn &cf, ReconstructFn &rf)
+  {
+    cf = condense_kernel<D, K>;
+    rf = reconstruct_kernel<D, K>;
+  }
+
+  bool
+  kernels_for(int dim, int k, CondenseFn &cf, ReconstructFn &rf)
+  {
+    switch (dim * 10 + k)
+      {
+        case 11: pick<1, 1>(cf, rf); return true;
+        case 12: pick<1, 2>(cf, rf); return true;
+        case 13: pick<1, 3>(cf, rf); return true;
+        case 21: pick<2, 1>(cf, rf); return true;
+        case 22: pick<2, 2>(cf, rf); return true;
+        case 23: pick<2, 3>(cf, rf); return true;
+        case 31: pick<3, 1>(cf, rf); return true;
+        case 32: pick<3, 2>(cf, rf); return true;
+        default: return false;
+      }
+  }
+
+  // warps per block, chunk size and table staging so that the workspace fits
+  // in the 227 KB of shared memory of a CTA
+  int
+  launch_shape(const ddhdg_ctx *c, const Mode &m, int &wpb, int &chunk, int &stage,
+               size_t &smem)
+  {
+    const size_t limit = 220 * 1024;
+    chunk              = 8;
+    const WsOff  w     = ws_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, chunk);
+    const size_t ws    = (size_t)w.total * sizeof(double);
+    const size_t tb    = (((size_t)c->to.total + 1) & ~(size_t)1) * sizeof(double);
+    for (stage = 1; stage >= 0; --stage)
+      for (wpb = 8; wpb >= 1; wpb /= 2)
+        {
+          smem = (stage ? tb : 0) + (size_t)wpb * ws;
+          if (smem <= limit)
+            return DDHDG_OK;
+        }
+    return fail(DDHDG_BAD_ARG, "the per-cell workspace does not fit in shared memory");
+  }
+
+  __global__ void
+  scatter_kernel(int64_t ncells, int F, int nf, int ncomp, int Nt, const double *tt,
+                 const double *rhs, const int32_t *dflag, const double *dval,
+                 const uint8_t *slots, const int32_t *rowptr, double *csr,
+                 double *grhs, int n0, int n1, const int64_t fo0, const int64_t fo1,
+                 const int64_t fo2, int e00, int e01, int e02, int e10, int e11,
+                 int e12, int e20, int e21, int e22, int dim)
+  {
+    const int64_t tot = ncells * (int64_t)Nt * Nt;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < tot;
+         idx += (int64_t)gridDim.x * blockDim.x)
+      {
+        const int64_t cell = idx / ((int64_t)Nt * Nt);
+        const int     i    = (int)((idx / Nt) % Nt);
+        const int     j    = (int)(idx % Nt);
+        const int     fi = i / (ncomp * nf), fj = j / (ncomp * nf);
+        int ci[3];
+        ci[0] = (int)(cell % n0);
+        ci[1] = (int)((cell / n0) % n1);
+        ci[2] = (int)(cell / ((int64_t)n0 * n1));
+        const int64_t off[3] = {fo0, fo1, fo2};
+        const int     ext[3][3] = {{e00, e01, e02}, {e10, e11, e12}, {e20, e21, e22}};
+        int           cf[3] = {ci[0], ci[1], ci[2]};
+        const int     a     = fi / 2;
+        cf[a] += fi % 2;
+        int64_t fidx = 0, stride = 1;
+        for (int b = 0; b < dim; ++b)
+          {
+            fidx += cf[b] * stride;
+            stride *= ext[a][b];
+          }
+        const int64_t Fi  = off[a] + fidx;
+        const int64_t row = Fi * ncomp * nf + (i % (ncomp * nf));
+        const int     sl  = slots[(cell * F + fi) * F + fj];
+        const int64_t pos = rowptr[row] + (int64_t)sl * ncomp * nf + (j % (ncomp * nf));
+        const double  v   = tt[idx];
+        if (v != 0.)
+          atomicAdd(csr + pos, v);
+        if (j == i && dflag[cell * Nt + i])
+          {
+            atomicAdd(csr + pos, 1.);
+            atomicAdd(grhs + row, dval[cell * Nt + i]);
+          }
+        else if (j == 0 && !dflag[cell * Nt + i])
+          atomicAdd(grhs + row, rhs[cell * Nt + i]);
+      }
+  }
+
+  __global__ void
+  gather_kernel(int64_t n, const int32_t *map, const double *src, double *dst)
+  {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+      dst[i] = src[map[i]];
+  }
+
+  __global__ void
+  scatter_perm_kernel(int64_t n, const int32_t *perm, const double *src, double *dst)
+  {
+    // dst[perm[i]] = src[i]
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+      dst[perm[i]] = src[i];
+  }
+
+  // restricted solution -> full trace update [nfaces][3][nf]
+  __global__ void
+  expand_kernel(int64_t nfaces, int nf, int ncomp, int c0, int c1, int c2,
+                const double *x, double *full)
+  {
+    const int     comps[3] = {c0, c1, c2};
+    const int64_t tot      = nfaces * 3 * nf;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot;
+         i += (int64_t)gridDim.x * blockDim.x)
+      {
+        const int64_t f = i / (3 * nf);
+        const int     b = (int)((i / nf) % 3);
+        const int     m = (int)(i % nf);
+        int           ce = -1;
+        for (int c = 0; c < ncomp; ++c)
+          if (comps[c] == b)
+            ce = c;
+        full[i] = (ce >= 0) ? x[(f * ncomp + ce) * nf + m] : 0.;
+      }
+  }
+
+  // out[0] = max|a|, out[1] = max|b|, out[2] = max|c|, out[3] = max|d|
+  __global__ void
+  absmax_kernel(const double *a, int64_t na, const double *b, int64_t nb_,
+                const double *c, int64_t nc, const double *d, int64_t nd,
+                unsigned long long *out)
+  {
+    double m[4] = {0., 0., 0., 0.};
+    const double *arr[4] = {a, b, c, d};
+    const int64_t n[4]   = {na, nb_, nc, nd};
+    for (int k = 0; k < 4; ++k)
+      for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n[k];
+           i += (int64_t)gridDim.x * blockDim.x)
+        {
+          const double v = fabs(arr[k][i]);
+          m[k]           = (v > m[k] || v != v) ? v : m[k];
+        }
+    for (int k = 0; k < 4; ++k)
+      {
+        double v = m[k];
+        for (int o = 16; o > 0; o >>= 1)
+          {
+            const double w = __shfl_xor_sync(0xffffffffu, v, o);
+            v              = (w != w || w > v) ? w : v; // keeps NaN
+          }
+        if ((threadIdx.x & 31) == 0)
+          atomicMax(out + k, __double_as_longlong(v));
+      }
+  }
+
+  __global__ void
+  axpy2_kernel(int64_t n1, double *y1, const double *x1, int64_t n2, double *y2,
+               const double *x2, double alpha)
+  {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n1 + n2;
+         i += (int64_t)gridDim.x * blockDim.x)
+      {
+        if (i < n1)
+          y1[i] += alpha * x1[i];
+        else
+          y2[i - n1] += alpha * x2[i - n1];
+      }
+  }
+
+  // L2 projection of point values into the scalar + weak-gradient flux
+  // coefficients of one component (src/project_component.cpp:268-420).
+  // mode 0: values given; mode 1: density of comp from the quasi Fermi
+  // potential qf and the cell's V (include/solver.h:378-412).
+  __global__ void
+  project_cell_kernel(int64_t ncells, int dim, int nb, int nqc, int nqf, int F,
+                      const double *tab, TabOff to, const double *vc, const double *vf,
+                      int comp, double *cell_state, int mode, double qf_pot,
+                      double T, double V_rescale, double n_rescale, double nband,
+                      double eband)
+  {
+    const double *phi_c  = tab + to.phi_c;
+    const double *grad_c = tab + to.grad_c;
+    const double *w_c    = tab + to.w_c;
+    const double *phi_f  = tab + to.phi_f;
+    const double *w_f    = tab + to.w_f;
+    const double *minv   = tab + to.minv;
+    const int     NCA    = 3 * (dim + 1) * nb;
+    for (int64_t cell = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; cell < ncells;
+         cell += (int64_t)gridDim.x * blockDim.x)
+      {
+        double       *cs = cell_state + cell * NCA;
+        const double *Vs = cs + (0 * (dim + 1) + dim) * nb;
+        double        rc[64], rd[3][64], val[64], valf[6][16];
+        for (int q = 0; q < nqc; ++q)
+          {
+            double v;
+            if (mode == 0)
+              v = vc[cell * nqc + q];
+            else
+              {
+                double V = 0.;
+                for (int a = 0; a < nb; ++a)
+                  V += phi_c[q * nb + a] * Vs[a];
+                V *= V_rescale;
+                const double kT = KB_ * T;
+                const double ex = (comp == 1) ? (Q_ * (V - qf_pot) - eband) / kT :
+                                                (Q_ * (qf_pot - V) + eband) / kT;
+                v               = nband * exp(ex) / n_rescale;
+              }
+            val[q] = v;
+          }
+        for (int f = 0; f < F; ++f)
+          for (int q = 0; q < nqf; ++q)
+            {
+              double v;
+              if (mode == 0)
+                v = vf[(cell * F + f) * nqf + q];
+              else
+                {
+                  double V = 0.;
+                  for (int a = 0; a < nb; ++a)
+                    V += phi_f[(f * nqf + q) * nb + a] * Vs[a];
+                  V *= V_rescale;
+                  const double kT = KB_ * T;
+                  const double ex = (comp == 1) ? (Q_ * (V - qf_pot) - eband) / kT :
+                                                  (Q_ * (qf_pot - V) + eband) / kT;
+                  v               = nband * exp(ex) / n_rescale;
+                }
+              valf[f][q] = v;
+            }
+        for (int b = 0; b < nb; ++b)
+          {
+            double acc = 0.;
+            for (int q = 0; q < nqc; ++q)
+              acc += w_c[q] * phi_c[q * nb + b] * val[q];
+            rc[b] = acc;
+            for (int s = 0; s < dim; ++s)
+              {
+                double ad = 0.;
+                for (int q = 0; q < nqc; ++q)
+                  ad += w_c[q] * grad_c[(q * nb + b) * dim + s] * val[q];
+                for (int f = 0; f < F; ++f)
+                  {
+                    if (f / 2 != s)
+                      continue;
+                    const double ns = (f & 1) ? 1. : -1.;
+                    for (int q = 0; q < nqf; ++q)
+                      ad -= ns * w_f[f * nqf + q] * phi_f[(f * nqf + q) * nb + b] * valf[f][q];
+                  }
+                rd[s][b] = ad;
+              }
+          }
+        double *blk = cs + comp * (dim + 1) * nb;
+        for (int a = 0; a < nb; ++a)
+          {
+            double u = 0.;
+            for (int b = 0; b < nb; ++b)
+              u += minv[a * nb + b] * rc[b];
+            blk[dim * nb + a] = u;
+            for (int s = 0; s < dim; ++s)
+              {
+                double w = 0.;
+                for (int b = 0; b < nb; ++b)
+                  w += minv[a * nb + b] * rd[s][b];
+                blk[s * nb + a] = w;
+              }
+          }
+      }
+  }
+
+  // L2 projection of face point values on the trace of comp.  mode 0:
+  // values [nfaces][nqf]; mode 1: l2_average of the two cells' values of comp
+  // (src/copy_on_trace.cpp:631-1010 with c_strategy 0).
+  __global__ void
+  project_trace_kernel(int64_t nfaces, int dim, int nb, int nf, int nqf, int F,
+                       const double *tab, TabOff to, const double *vals, int comp,
+                       double *trace_state, int mode, const double *cell_state,
+                       const int64_t *face_cells, const int64_t *cell_face_local)
+  {
+    const double *phi_f  = tab + to.phi_f;
+    const double *fminvw = tab + to.fminvw;
+    const int     NCA    = 3 * (dim + 1) * nb;
+    for (int64_t Fi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; Fi < nfaces;
+         Fi += (int64_t)gridDim.x * blockDim.x)
+      {
+        double v[16];
+        for (int q = 0; q < nqf; ++q)
+          v[q] = 0.;
+        if (mode == 0)
+          for (int q = 0; q < nqf; ++q)
+            v[q] = vals[Fi * nqf + q];
+        else
+          {
+            int cnt = 0;
+            for (int sd = 0; sd < 2; ++sd)
+              {
+                const int64_t cell = face_cells[Fi * 2 + sd];
+                if (cell < 0)
+                  continue;
+                ++cnt;
+                const int     f  = (int)cell_face_local[Fi * 2 + sd];
+                const double *cs = cell_state + cell * NCA + (comp * (dim + 1) + dim) * nb;
+                for (int q = 0; q < nqf; ++q)
+                  {
+                    double u = 0.;
+                    for (int a = 0; a < nb; ++a)
+                      u += phi_f[(f * nqf + q) * nb + a] * cs[a];
+                    v[q] += u;
+                  }
+              }
+            for (int q = 0; q < nqf; ++q)
+              v[q] /= cnt;
+          }
+        for (int m = 0; m < nf; ++m)
+          {
+            double acc = 0.;
+            for (int q = 0; q < nqf; ++q)
+              acc += fminvw[m * nqf + q] * v[q];
+            trace_state[(Fi * 3 + comp) * nf + m] = acc;
+          }
+      }
+  }
+
+  int
+  grid_for(const ddhdg_ctx *c, int64_t work, int block)
+  {
+    int64_t g = (work + block - 1) / block;
+    g         = std::min<int64_t>(g, (int64_t)c->sm_count * 32);
+    return (int)std::max<int64_t>(g, 1);
+  }
+} // namespace
+
+extern "C" {
+
+const char *
+ddhdg_last_error(void)
+{
+  return g_last_error.c_str();
+}
+
+int
+ddhdg_reference_points(int dim, int degree, double *qref_c, double *qref_f, double *support)
+{
+  if (dim < 1 || dim > 3 || degree < 0 || degree > 6)
+    return fail(DDHDG_BAD_ARG, "bad dim/degree");
+  const double h[3] = {1., 1., 1.};
+  const Tables T    = build_tables(dim, degree, h);
+  if (qref_c)
+    std::copy(T.qref_c.begin(), T.qref_c.end(), qref_c);
+  if (qref_f)
+    std::copy(T.qref_f.begin(), T.qref_f.end(), qref_f);
+  if (support)
+    std::copy(T.gl.begin(), T.gl.end(), support);
+  return DDHDG_OK;
+}
+
+int
+ddhdg_ctx_create(const ddhdg_problem_desc *d, ddhdg_ctx **out)
+{
+  if (!d || !out)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  *out = nullptr;
+  if (d->dim < 1 || d->dim > 3 || d->degree < 1 || d->degree > 3)
+    return fail(DDHDG_BAD_ARG, "dim must be 1..3 and degree 1..3");
+  if (d->dim == 3 && d->degree > 2)
+    return fail(DDHDG_BAD_ARG, "3D supports degree 1 and 2");
+  for (int a = 0; a < d->dim; ++a)
+    if (d->n[a] < 1 || !(d->h[a] > 0.))
+      return fail(DDHDG_BAD_ARG, "bad mesh");
+  if (!d->doping_host || !d->face_bc_host || !d->face_bc_val_host)
+    return fail(DDHDG_BAD_ARG, "doping and boundary tables are required");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    {
+      cudaGetLastError();
+      return fail(DDHDG_NO_DEVICE, "no CUDA device");
+    }
+  auto c  = std::make_unique<ddhdg_ctx>();
+  c->desc = *d;
+  c->dim  = d->dim;
+  c->k    = d->degree;
+  c->T    = build_tables(d->dim, d->degree, d->h);
+  c->nb   = c->T.nb;
+  c->nf   = c->T.nf;
+  c->nqc  = c->T.nqc;
+  c->nqf  = c->T.nqf;
+  c->F    = c->T.F;
+  for (int b = 0; b < 3; ++b)
+    c->enabled[b] = d->enabled[b] ? 1 : 0;
+  c->ncells = 1;
+  for (int a = 0; a < d->dim; ++a)
+    c->ncells *= d->n[a];
+  int64_t off = 0;
+  for (int a = 0; a < d->dim; ++a)
+    {
+      c->face_off[a] = off;
+      int64_t cnt    = 1;
+      for (int b = 0; b < 3; ++b)
+        {
+          const int e      = (b < d->dim) ? (d->n[b] + (b == a ? 1 : 0)) : 1;
+          c->face_ext[a][b] = e;
+          cnt *= e;
+        }
+      off += cnt;
+    }
+  c->nfaces = off;
+  // face -> cells
+  c->face_cells.assign(c->nfaces * 2, -1);
+  for (int64_t cell = 0; cell < c->ncells; ++cell)
+    for (int f = 0; f < c->F; ++f)
+      {
+        const int64_t Fi            = face_of_cell(c.get(), cell, f);
+        c->face_cells[Fi * 2 + (1 - f % 2)] = cell;
+      }
+  {
+    std::vector<int64_t> loc(c->nfaces * 2, -1);
+    for (int64_t cell = 0; cell < c->ncells; ++cell)
+      for (int f = 0; f < c->F; ++f)
+        loc[face_of_cell(c.get(), cell, f) * 2 + (1 - f % 2)] = f;
+    int r0;
+    if ((r0 = c->d_face_cells.upload(c->face_cells.data(), c->face_cells.size())))
+      return r0;
+    if ((r0 = c->d_face_local.upload(loc.data(), loc.size())))
+      return r0;
+  }
+  // stage the tables in one block
+  {
+    std::vector<double> blob;
+    auto put = [&](const std::vector<double> &v) {
+      int o = (int)blob.size();
+      blob.insert(blob.end(), v.begin(), v.end());
+      while (blob.size() % 2)
+        blob.push_back(0.);
+      return o;
+    };
+    c->to.phi_c  = put(c->T.phi_c);
+    c->to.grad_c = put(c->T.grad_c);
+    c->to.w_c    = put(c->T.w_c);
+    c->to.phi_f  = put(c->T.phi_f);
+    c->to.w_f    = put(c->T.w_f);
+    c->to.xi     = put(c->T.xi);
+    c->to.fminvw = put(c->T.fminvw);
+    c->to.PW_c   = put(c->T.PW_c);
+    c->to.PW_f   = put(c->T.PW_f);
+    c->to.QW_c   = put(c->T.QW_c);
+    c->to.QW_f   = put(c->T.QW_f);
+    c->to.P      = put(c->T.P);
+    c->to.Q      = put(c->T.Q);
+    c->to.minv   = put(c->T.minv);
+    c->to.total  = (int)blob.size();
+    int r        = c->tables.upload(blob.data(), blob.size());
+    if (r)
+      return r;
+  }
+  int r;
+  const int64_t nq = c->ncells * c->nqc;
+  if ((r = c->doping.upload(d->doping_host, nq)))
+    return r;
+  if (d->rec_a_host && (r = c->rec_a.upload(d->rec_a_host, nq)))
+    return r;
+  if (d->rec_b_host && (r = c->rec_b.upload(d->rec_b_host, nq)))
+    return r;
+  if (d->rec_c_host && (r = c->rec_c.upload(d->rec_c_host, nq)))
+    return r;
+  if (d->tau_host && (r = c->tau_table.upload(d->tau_host, c->ncells * c->F * 3)))
+    return r;
+  if ((r = c->bc.upload(d->face_bc_host, c->nfaces * 3)))
+    return r;
+  if ((r = c->bc_val.upload(d->face_bc_val_host, c->nfaces * 3 * c->nqf)))
+    return r;
+  if ((r = c->status.alloc(1)))
+    return r;
+  CK(cudaMemset(c->status.p, 0, sizeof(int)));
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, dev));
+  // host pointers are not kept
+  c->desc.doping_host = nullptr;
+  c->desc.rec_a_host = c->desc.rec_b_host = c->desc.rec_c_host = nullptr;
+  c->desc.tau_host                                             = nullptr;
+  c->desc.face_bc_host                                         = nullptr;
+  c->desc.face_bc_val_host                                     = nullptr;
+  *out = c.release();
+  return DDHDG_OK;
+}
+
+int
+ddhdg_ctx_destroy(ddhdg_ctx *c)
+{
+  if (!c)
+    return DDHDG_OK;
+  if (c->sp)
+    cusolverSpDestroy(c->sp);
+  if (c->descr)
+    cusparseDestroyMatDescr(c->descr);
+  delete c;
+  return DDHDG_OK;
+}
+
+int
+ddhdg_get_sizes(const ddhdg_ctx *cc, int thermo, ddhdg_sizes *s)
+{
+  if (!cc || !s)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  ddhdg_ctx *c = const_cast<ddhdg_ctx *>(cc);
+  thermo       = thermo ? 1 : 0;
+  int r;
+  if (!c->mode[thermo].built && (r = build_mode(c, thermo)))
+    return r;
+  const Mode &m  = c->mode[thermo];
+  s->ncells      = c->ncells;
+  s->nfaces      = c->nfaces;
+  s->Nc_all      = 3 * (c->dim + 1) * c->nb;
+  s->Nt          = m.Nt;
+  s->ncomp       = m.ncomp;
+  s->nqc         = c->nqc;
+  s->nqf         = c->nqf;
+  s->nb          = c->nb;
+  s->nf          = c->nf;
+  s->n_trace_dofs = m.ndofs;
+  s->nnz         = m.nnz;
+  return DDHDG_OK;
+}
+
+int
+ddhdg_set_boundary(ddhdg_ctx *c, const int32_t *bc, const double *val)
+{
+  if (!c || !bc || !val)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  int r;
+  if ((r = c->bc.upload(bc, c->nfaces * 3)))
+    return r;
+  return c->bc_val.upload(val, c->nfaces * 3 * c->nqf);
+}
+
+int
+ddhdg_set_enabled(ddhdg_ctx *c, int V, int n, int p)
+{
+  if (!c)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  if (!V && !n && !p)
+    return fail(DDHDG_BAD_ARG, "no component enabled");
+  const int nv[3] = {V ? 1 : 0, n ? 1 : 0, p ? 1 : 0};
+  if (nv[0] != c->enabled[0] || nv[1] != c->enabled[1] || nv[2] != c->enabled[2])
+    {
+      for (int b = 0; b < 3; ++b)
+        c->enabled[b] = nv[b];
+      c->mode[0].built = false;
+    }
+  return DDHDG_OK;
+}
+
+int
+ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
+                        const double *trace_state, int thermo, double *tt,
+                        double *rhs, int32_t *dflag, double *dval,
+                        ddhdg_stream_t stream)
+{
+  if (!c || !cell_state || !trace_state || !tt || !rhs || !dflag || !dval)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo = thermo ? 1 : 0;
+  int r;
+  if ((r = ensure_buffers(c, thermo)))
+    return r;
+  Mode      &m = c->mode[thermo];
+  CondenseFn cf;
+  ReconstructFn rf;
+  if (!kernels_for(c->dim, c->k, cf, rf))
+    return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
+  KParams P     = make_params(c, thermo);
+  P.cell_state  = cell_state;
+  P.trace_state = trace_state;
+  P.tt          = tt;
+  P.rhs         = rhs;
+  P.dflag       = dflag;
+  P.dval        = dval;
+  P.ycache      = m.ycache.p;
+  int    wpb, chunk, stage;
+  size_t smem;
+  if ((r = launch_shape(c, m, wpb, chunk, stage, smem)))
+    return r;
+  P.wpb   = wpb;
+  P.chunk = chunk;
+  P.stage = stage;
+  CK(cudaFuncSetAttribute(cf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, wpb * 32, smem));
+  if (per_sm < 1)
+    return fail(DDHDG_BAD_ARG, "condense kernel does not fit on an SM");
+  const int64_t blocks_needed = (c->ncells + wpb - 1) / wpb;
+  const int     grid = (int)std::min<int64_t>(blocks_needed, (int64_t)per_sm * c->sm_count);
+  cf<<<grid, wpb * 32, smem, (cudaStream_t)stream>>>(P);
+  CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+int
+ddhdg_reconstruct(ddhdg_ctx *c, const double *cell_state, const double *trace_state,
+                  const double *update_trace, double *update_cell, int thermo,
+                  ddhdg_stream_t stream)
+{
+  if (!c || !cell_state || !trace_state || !update_trace || !update_cell)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo = thermo ? 1 : 0;
+  Mode &m = c->mode[thermo];
+  if (!m.built || !m.ycache.p)
+    return fail(DDHDG_BAD_ARG, "ddhdg_reconstruct needs a preceding ddhdg_assemble_condense");
+  CondenseFn    cf;
+  ReconstructFn rf;
+  if (!kernels_for(c->dim, c->k, cf, rf))
+    return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
+  KParams P     = make_params(c, thermo);
+  P.cell_state  = cell_state;
+  P.trace_state = trace_state;
+  P.ycache      = m.ycache.p;
+  const int    Ns  = m.ncomp * c->nb;
+  const int    wsz = (Ns + 2 * c->F * 3 * c->nf + c->nb + 1) & ~1;
+  const int    wpb = 8;
+  const size_t nPQ = (size_t)(c->to.minv - c->to.P);
+  const size_t smem =
+    ((nPQ + 1) & ~(size_t)1) * sizeof(double) + (size_t)wpb * wsz * sizeof(double);
+  P.wpb = wpb;
+  CK(cudaFuncSetAttribute(rf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rf, wpb * 32, smem));
+  const int64_t blocks_needed = (c->ncells + wpb - 1) / wpb;
+  const int     grid =
+    (int)std::max<int64_t>(1, std::min<int64_t>(blocks_needed, (int64_t)std::max(per_sm, 1) * c->sm_count));
+  rf<<<grid, wpb * 32, smem, (cudaStream_t)stream>>>(P, update_trace, update_cell);
+  CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+int
+ddhdg_get_csr(ddhdg_ctx *c, int thermo, const int32_t **row_ptr, const int32_t **col_idx)
+{
+  if (!c || !row_ptr || !col_idx)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo = thermo ? 1 : 0;
+  int r;
+  if (!c->mode[thermo].built && (r = build_mode(c, thermo)))
+    return r;
+  *row_ptr = c->mode[thermo].rowptr.p;
+  *col_idx = c->mode[thermo].colind.p;
+  return DDHDG_OK;
+}
+
+int
+ddhdg_scatter(ddhdg_ctx *c, const double *tt, const double *rhs, const int32_t *dflag,
+              const double *dval, double *csr, double *grhs, int thermo,
+              ddhdg_stream_t stream)
+{
+  if (!c || !tt || !rhs || !dflag || !dval || !csr || !grhs)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo  = thermo ? 1 : 0;
+  Mode &m = c->mode[thermo];
+  int   r;
+  if (!m.built && (r = build_mode(c, thermo)))
+    return r;
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(csr, 0, m.nnz * sizeof(double), s));
+  CK(cudaMemsetAsync(grhs, 0, m.ndofs * sizeof(double), s));
+  const int64_t tot = c->ncells * (int64_t)m.Nt * m.Nt;
+  scatter_kernel<<<grid_for(c, tot, 256), 256, 0, s>>>(
+    c->ncells, c->F, c->nf, m.ncomp, m.Nt, tt, rhs, dflag, dval, m.slots.p,
+    m.rowptr.p, csr, grhs, c->desc.n[0], c->dim > 1 ? c->desc.n[1] : 1,
+    c->face_off[0], c->face_off[1], c->face_off[2], c->face_ext[0][0],
+    c->face_ext[0][1], c->face_ext[0][2], c->face_ext[1][0], c->face_ext[1][1],
+    c->face_ext[1][2], c->face_ext[2][0], c->face_ext[2][1], c->face_ext[2][2], c->dim);
+  CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+int
+ddhdg_solve_trace(ddhdg_ctx *c, const double *csr, const double *grhs, double *x,
+                  int thermo, ddhdg_stream_t stream)
+{
+  if (!c || !csr || !grhs || !x)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo  = thermo ? 1 : 0;
+  Mode &m = c->mode[thermo];
+  if (!m.built)
+    return fail(DDHDG_BAD_ARG, "sparsity not built");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!c->sp)
+    {
+      if (cusolverSpCreate(&c->sp) != CUSOLVER_STATUS_SUCCESS)
+        return fail(DDHDG_SOLVER_ERROR, "cusolverSpCreate failed");
+      if (cusparseCreateMatDescr(&c->descr) != CUSPARSE_STATUS_SUCCESS)
+        return fail(DDHDG_SOLVER_ERROR, "cusparseCreateMatDescr failed");
+      cusparseSetMatType(c->descr, CUSPARSE_MATRIX_TYPE_GENERAL);
+      cusparseSetMatIndexBase(c->descr, CUSPARSE_INDEX_BASE_ZERO);
+    }
+  cusolverSpSetStream(c->sp, s);
+  int r;
+  if ((r = m.pval.alloc(m.nnz)) || (r = m.pb.alloc(m.ndofs)) || (r = m.px.alloc(m.ndofs)))
+    return r;
+  // B = A(perm, perm), pb = b(perm)
+  gather_kernel<<<grid_for(c, m.nnz, 256), 256, 0, s>>>(m.nnz, m.pmap.p, csr, m.pval.p);
+  gather_kernel<<<grid_for(c, m.ndofs, 256), 256, 0, s>>>(m.ndofs, m.d_perm.p, grhs, m.pb.p);
+  CK(cudaGetLastError());
+  int sing = -1;
+  const cusolverStatus_t st = cusolverSpDcsrlsvqr(
+    c->sp, (int)m.ndofs, (int)m.nnz, c->descr, m.pval.p, m.prow.p, m.pcol.p, m.pb.p,
+    1e-14, 0, m.px.p, &sing);
+  if (st != CUSOLVER_STATUS_SUCCESS)
+    return fail(DDHDG_SOLVER_ERROR, "cusolverSpDcsrlsvqr failed with status " + std::to_string((int)st));
+  if (sing >= 0)
+    return fail(DDHDG_SOLVER_ERROR, "global trace matrix is singular at row " + std::to_string(sing));
+  // x = px(iperm): x[perm[i]] = px[i]
+  scatter_perm_kernel<<<grid_for(c, m.ndofs, 256), 256, 0, s>>>(m.ndofs, m.d_perm.p, m.px.p, x);
+  CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+int
+ddhdg_newton(ddhdg_ctx *c, double *cell_state, double *trace_state, int thermo,
+             double abs_tol, double rel_tol, int max_it, double alpha, int *iterations,
+             double *last_update_norm, ddhdg_stream_t stream)
+{
+  if (!c || !cell_state || !trace_state)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo = thermo ? 1 : 0;
+  int r;
+  if ((r = ensure_buffers(c, thermo)))
+    return r;
+  Mode         &m       = c->mode[thermo];
+  cudaStream_t  s       = (cudaStream_t)stream;
+  const int64_t ncell_d = c->ncells * 3 * (c->dim + 1) * c->nb;
+  const int64_t ntr_d   = c->nfaces * 3 * c->nf;
+  if ((r = m.csr.alloc(m.nnz)) || (r = m.grhs.alloc(m.ndofs)) || (r = m.x.alloc(m.ndofs)) ||
+      (r = m.dtrace.alloc(ntr_d)) || (r = m.dcell.alloc(ncell_d)) ||
+      (r = c->norm_buf.alloc(4)))
+    return r;
+  cudaEvent_t ev[4];
+  for (auto &e : ev)
+    CK(cudaEventCreate(&e));
+  c->t_condense = c->t_solve = c->t_recon = 0.;
+  c->t_steps                              = 0;
+  bool   converged                        = false;
+  int    step                             = 0;
+  double upd_cell_norm                    = 0.;
+  CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), s));
+  int rc = DDHDG_OK;
+  while (max_it < 0 || step < max_it)
+    {
+      ++step;
+      CK(cudaEventRecord(ev[0], s));
+      if ((rc = ddhdg_assemble_condense(c, cell_state, trace_state, thermo, m.tt.p, m.rhs.p,
+                                        m.dflag.p, m.dval.p, stream)))
+        break;
+      if ((rc = ddhdg_scatter(c, m.tt.p, m.rhs.p, m.dflag.p, m.dval.p, m.csr.p, m.grhs.p,
+                              thermo, stream)))
+        break;
+      CK(cudaEventRecord(ev[1], s));
+      if ((rc = ddhdg_solve_trace(c, m.csr.p, m.grhs.p, m.x.p, thermo, stream)))
+        break;
+      expand_kernel<<<grid_for(c, ntr_d, 256), 256, 0, s>>>(
+        c->nfaces, c->nf, m.ncomp, m.comps[0], m.comps[1], m.comps[2], m.x.p, m.dtrace.p);
+      CK(cudaEventRecord(ev[2], s));
+      if ((rc = ddhdg_reconstruct(c, cell_state, trace_state, m.dtrace.p, m.dcell.p, thermo,
+                                  stream)))
+        break;
+      CK(cudaEventRecord(ev[3], s));
+      // norms: |dcell|, |dtrace|, |cell|, |trace| (before the update)
+      CK(cudaMemsetAsync(c->norm_buf.p, 0, 4 * sizeof(double), s));
+      absmax_kernel<<<grid_for(c, ncell_d, 256), 256, 0, s>>>(
+        m.dcell.p, ncell_d, m.dtrace.p, ntr_d, cell_state, ncell_d, trace_state, ntr_d,
+        reinterpret_cast<unsigned long long *>(c->norm_buf.p));
+      axpy2_kernel<<<grid_for(c, ncell_d + ntr_d, 256), 256, 0, s>>>(
+        ntr_d, trace_state, m.dtrace.p, ncell_d, cell_state, m.dcell.p, alpha);
+      CK(cudaGetLastError());
+      double nrm[4];
+      int    status = 0;
+      CK(cudaMemcpyAsync(nrm, c->norm_buf.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(&status, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      float t01, t12, t23;
+      cudaEventElapsedTime(&t01, ev[0], ev[1]);
+      cudaEventElapsedTime(&t12, ev[1], ev[2]);
+      cudaEventElapsedTime(&t23, ev[2], ev[3]);
+      c->t_condense += t01;
+      c->t_solve += t12;
+      c->t_recon += t23;
+      c->t_steps += 1;
+      if (status)
+        {
+          rc = fail(status, "a local cell system had a zero or non-finite pivot");
+          break;
+        }
+      upd_cell_norm            = nrm[0];
+      const double update_norm = std::max(nrm[0], nrm[1]);
+      const double cur_norm    = std::max(nrm[2], nrm[3]);
+      if (!std::isfinite(update_norm))
+        {
+          rc = fail(DDHDG_NOT_CONVERGED, "non-finite Newton update");
+          break;
+        }
+      if (update_norm < abs_tol || update_norm < rel_tol * cur_norm)
+        {
+          converged = true;
+          break;
+        }
+    }
+  for (auto &e : ev)
+    cudaEventDestroy(e);
+  if (iterations)
+    *iterations = step;
+  if (last_update_norm)
+    *last_update_norm = upd_cell_norm;
+  if (rc)
+    return rc;
+  return converged ? DDHDG_OK : DDHDG_NOT_CONVERGED;
+}
+
+int
+ddhdg_last_timings(const ddhdg_ctx *c, double *a, double *b, double *d, int *steps)
+{
+  if (!c)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  if (a)
+    *a = c->t_condense;
+  if (b)
+    *b = c->t_solve;
+  if (d)
+    *d = c->t_recon;
+  if (steps)
+    *steps = c->t_steps;
+  return DDHDG_OK;
+}
+
+int
+ddhdg_project_cell(ddhdg_ctx *c, const double *vals_cell, const double *vals_face, int comp,
+                   double *cell_state, ddhdg_stream_t stream)
+{
+  if (!c || !vals_cell || !vals_face || !cell_state || comp < 0 || comp > 2)
+    return fail(DDHDG_BAD_ARG, "bad argument");
+  if (c->nb > 64 || c->nqf > 16)
+    return fail(DDHDG_BAD_ARG, "projection supports (k+1)^d <= 64");
+  project_cell_kernel<<<grid_for(c, c->ncells, 128), 128, 0, (cudaStream_t)stream>>>(
+    c->ncells, c->dim, c->nb, c->nqc, c->nqf, c->F, c->tables.p, c->to, vals_cell, vals_face,
+    comp, cell_state, 0, 0., 0., 0., 0., 0., 0.);
+  CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+int
+ddhdg_project_trace(ddhdg_ctx *c, const double *vals_face, int comp, double *trace_state,
+                    ddhdg_stream_t stream)
+{
+  if (!c || !vals_face || !trace_state || comp < 0 || comp > 2)
+    return fail(DDHDG_BAD_ARG, "bad argument");
+  project_trace_kernel<<<grid_for(c, c->nfaces, 128), 128, 0, (cudaStream_t)stream>>>(
+    c->nfaces, c->dim, c->nb, c->nf, c->nqf, c->F, c->tables.p, c->to, vals_face, comp,
+    trace_state, 0, nullptr, nullptr, nullptr);
+  CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+int
+ddhdg_project_density(ddhdg_ctx *c, int comp, double qf, double *cell_state,
+                      double *trace_state, ddhdg_stream_t stream)
+{
+  if (!c || !cell_state || !trace_state || (comp != 1 && comp != 2))
+    return fail(DDHDG_BAD_ARG, "bad argument");
+  if (c->nb > 64 || c->nqf > 16)
+    return fail(DDHDG_BAD_ARG, "projection supports (k+1)^d <= 64");
+  const auto  &d     = c->desc;
+  const double nband = (comp == 1) ? d.nc : d.nv;
+  const double eband = ((comp == 1) ? d.ec_eV : d.ev_eV) * EV_;
+  project_cell_kernel<<<grid_for(c, c->ncells, 128), 128, 0, (cudaStream_t)stream>>>(
+    c->ncells, c->dim, c->nb, c->nqc, c->nqf, c->F, c->tables.p, c->to, nullptr, nullptr, comp,
+    cell_state, 1, qf, d.temperature, d.V_rescale, d.n_rescale, nband, eband);
+  project_trace_kernel<<<grid_for(c, c->nfaces, 128), 128, 0, (cudaStream_t)stream>>>(
+    c->nfaces, c->dim, c->nb, c->nf, c->nqf, c->F, c->tables.p, c->to, nullptr, comp,
+    trace_state, 1, cell_state, c->d_face_cells.p, c->d_face_local.p);
+  CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+} // extern "C"

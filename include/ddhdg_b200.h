@@ -1,0 +1,228 @@
+/* ddhdg_b200 -- C ABI of the B200 (sm_100a) HDG hot path for the Van
+ * Roosbroeck drift-diffusion system.
+ *
+ * The library replaces, for structured Cartesian meshes of segments, quads
+ * and hexes, the per-Newton-step work that the reference (spiani/ddhdg) does
+ * in
+ *   NPSolver<dim,Problem>::assemble_system(reconstruct, thermo_eq, mt)
+ *       include/np_solver.h:627-630, include/assembling_methods.template.h:10-89
+ *   the per-cell worker assemble_system_one_cell<...>
+ *       include/assembling_methods.template.h:2290-2748
+ *   LocalCondenser::condense_ct_matrix   src/local_condenser.cpp:142-160
+ *   copy_local_to_global                 src/np_solver.cpp:1293-1322
+ *   the Newton loop private_run          src/np_solver.cpp:1452-1561
+ *
+ * Conventions
+ *   - Every entry point returns an int status (DDHDG_OK == 0); no C++
+ *     exception crosses the boundary.
+ *   - Arrays are device pointers owned by the caller unless the name of the
+ *     argument ends in _host.
+ *   - Cells are numbered lexicographically (x fastest).  The degrees of
+ *     freedom of cell c are contiguous: cell_state[c * Nc_all + ...] with the
+ *     per-cell order [E_0..E_{d-1}, V, Wn_0.., n, Wp_0.., p] x (k+1)^d
+ *     Gauss-Lobatto nodes (x fastest) -- the FESystem order of the
+ *     reference's FE_DGQ spaces (src/np_solver.cpp:292-325).
+ *   - Faces are numbered axis by axis (all x-normal faces, then y, then z),
+ *     lexicographically inside each axis.  The full trace vector is
+ *     trace_state[F][3][nf] (components V, n, p; (k+1)^(d-1) Gauss-Lobatto
+ *     nodes of FE_FaceQ).  The restricted trace system (enabled components
+ *     only) numbers dof (F, comp, m) as (F * ncomp + comp) * nf + m.
+ *   - All physical quantities are already rescaled by the Adimensionalizer
+ *     (include/adimensionalizer.h:28-262) except the band data and the SRH
+ *     intrinsic density, which the kernels rescale like the reference.
+ */
+#ifndef DDHDG_B200_H
+#define DDHDG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *ddhdg_stream_t; /* a cudaStream_t */
+
+enum ddhdg_status
+{
+  DDHDG_OK             = 0,
+  DDHDG_BAD_ARG        = 1,
+  DDHDG_OOM            = 2,
+  DDHDG_SINGULAR_PIVOT = 3, /* a local (cell) factorisation met a zero pivot */
+  DDHDG_REFINE_STALLED = 4, /* mixed precision refinement did not converge */
+  DDHDG_TIMEOUT        = 5,
+  DDHDG_CUDA_ERROR     = 6,
+  DDHDG_NOT_CONVERGED  = 7, /* Newton reached the iteration cap */
+  DDHDG_SOLVER_ERROR   = 8, /* the global trace solve failed */
+  DDHDG_NO_DEVICE      = 9
+};
+
+enum ddhdg_flux
+{
+  DDHDG_FLUX_USE_CELL  = 0, /* DDFluxType::use_cell */
+  DDHDG_FLUX_USE_TRACE = 1, /* DDFluxType::use_trace */
+  DDHDG_FLUX_QIU_SHI   = 2  /* DDFluxType::qiu_shi_stabilization */
+};
+
+enum ddhdg_bc
+{
+  DDHDG_BC_NONE      = 0,
+  DDHDG_BC_DIRICHLET = 1,
+  DDHDG_BC_NEUMANN   = 2
+};
+
+/* Problem description (host memory; copied to the device by
+ * ddhdg_ctx_create).  Mirrors Ddhdg::Problem (include/problem.h:13-46) with
+ * the solver parameters (include/np_solver_parameters.h:261-404). */
+typedef struct ddhdg_problem_desc
+{
+  int    dim;    /* 1, 2 or 3 */
+  int    degree; /* polynomial degree k of V, n and p (cell and trace) */
+  int    n[3];   /* cells per axis */
+  double origin[3];
+  double h[3];   /* cell size per axis in mesh units */
+
+  int enabled[3]; /* V, n, p */
+  int flux;       /* enum ddhdg_flux */
+  int phi_linearize;
+  /* bit 0: consistent sign of the E coupling in the cell drift terms;
+   * bit 1: recombination derivatives scaled by the doping magnitude.
+   * 0 reproduces the reference's Jacobian exactly. */
+  int jacobian_fix;
+  int precision; /* 0: FP64, 1: FP32 local factorisation + FP64 residuals */
+
+  double eps;         /* rescaled permittivity */
+  double mu_n, mu_p;  /* rescaled mobilities */
+  double temperature; /* kelvin (constant over the device) */
+  double thermal_voltage_rescale;
+  double V_rescale, n_rescale, rec_rescale;
+  double nc, nv, ec_eV, ev_eV; /* band densities and edges (physical) */
+
+  int    rec_type; /* 0: linear a + (b n + c p), 1: SRH fixed temperature */
+  double srh_ni, srh_tau_n, srh_tau_p;
+  const double *rec_a_host, *rec_b_host, *rec_c_host; /* [ncells*nqc] or NULL */
+
+  const double *doping_host; /* [ncells*nqc] rescaled doping at cell qps */
+  double        tau[3];      /* fixed tau per component (rescaled) */
+  const double *tau_host;    /* [ncells*2*dim*3] per cell/face tau, or NULL */
+  const int32_t *face_bc_host;   /* [nfaces*3] enum ddhdg_bc */
+  const double  *face_bc_val_host; /* [nfaces*3*nqf] rescaled BC data */
+} ddhdg_problem_desc;
+
+typedef struct ddhdg_ctx ddhdg_ctx;
+
+typedef struct ddhdg_sizes
+{
+  int64_t ncells, nfaces;
+  int     Nc_all; /* cell dofs per cell (all components) */
+  int     Nt;     /* restricted trace dofs per cell */
+  int     ncomp;  /* enabled components */
+  int     nqc, nqf, nb, nf;
+  int64_t n_trace_dofs; /* restricted global trace dofs */
+  int64_t nnz;          /* nonzeros of the global trace matrix */
+} ddhdg_sizes;
+
+/* NPSolver construction + setup_overall_system (src/np_solver.cpp:553-655):
+ * geometry tables, coefficient tables, trace sparsity.  Replaces
+ * NPSolver::NPSolver + setup_overall_system + setup_restricted_trace_system. */
+int ddhdg_ctx_create(const ddhdg_problem_desc *desc, ddhdg_ctx **ctx);
+int ddhdg_ctx_destroy(ddhdg_ctx *ctx);
+int ddhdg_get_sizes(const ddhdg_ctx *ctx, int thermo_eq, ddhdg_sizes *out);
+
+/* replace_boundary_condition (src/np_solver.cpp:2160-2233): new BC types and
+ * data for every face; the sparsity is unchanged. */
+int ddhdg_set_boundary(ddhdg_ctx *ctx, const int32_t *face_bc_host,
+                       const double *face_bc_val_host);
+/* set_enabled_components (src/np_solver.cpp:1064-1093). */
+int ddhdg_set_enabled(ddhdg_ctx *ctx, int V, int n, int p);
+
+/* assemble_system(false, thermo_eq) per-cell part: for every cell, assemble
+ * the local HDG system and condense it onto the cell's trace dofs
+ * (include/assembling_methods.template.h:2290-2686).  Outputs per cell:
+ *   tt   [ncells][Nt][Nt]  condensed trace matrix, Dirichlet rows/cols zero
+ *   rhs  [ncells][Nt]      condensed right-hand side
+ *   dflag[ncells][Nt]      1 where the trace dof is Dirichlet-constrained
+ *   dval [ncells][Nt]      projected Dirichlet increment (T:1592-1691)
+ * The cell's reconstruction data stays in the context for ddhdg_reconstruct.
+ * cell_state [ncells][Nc_all], trace_state [nfaces][3][nf] on the device. */
+int ddhdg_assemble_condense(ddhdg_ctx *ctx, const double *cell_state,
+                            const double *trace_state, int thermo_eq,
+                            double *tt, double *rhs, int32_t *dflag,
+                            double *dval, ddhdg_stream_t stream);
+
+/* copy_local_to_global (src/np_solver.cpp:1293-1322): scatter the per-cell
+ * condensed systems into the global CSR trace matrix (values[nnz], rows and
+ * columns from ddhdg_get_csr) and rhs[n_trace_dofs]; Dirichlet rows become
+ * identity rows whose rhs is the constrained value. */
+int ddhdg_scatter(ddhdg_ctx *ctx, const double *tt, const double *rhs,
+                  const int32_t *dflag, const double *dval, double *csr_values,
+                  double *global_rhs, int thermo_eq, ddhdg_stream_t stream);
+/* Global trace sparsity (device arrays owned by the context). */
+int ddhdg_get_csr(ddhdg_ctx *ctx, int thermo_eq, const int32_t **row_ptr,
+                  const int32_t **col_idx);
+
+/* solve_linear_problem (src/np_solver.cpp:1326-1354) on the device:
+ * x = A^-1 b for the global trace system (cuSOLVER sparse QR). */
+int ddhdg_solve_trace(ddhdg_ctx *ctx, const double *csr_values,
+                      const double *global_rhs, double *x, int thermo_eq,
+                      ddhdg_stream_t stream);
+
+/* assemble_system(true, thermo_eq): cell update from the full trace update
+ * update_trace [nfaces][3][nf] (include/assembling_methods.template.h:
+ * 2122-2160 and 2688-2697).  Uses the reconstruction data kept by the last
+ * ddhdg_assemble_condense on the same state. */
+int ddhdg_reconstruct(ddhdg_ctx *ctx, const double *cell_state,
+                      const double *trace_state, const double *update_trace,
+                      double *update_cell, int thermo_eq,
+                      ddhdg_stream_t stream);
+
+/* private_run (src/np_solver.cpp:1452-1561) on device-resident state:
+ * Newton iterations with damping alpha, absolute / relative stop on the
+ * infinity norm of the update.  cell_state / trace_state are updated in
+ * place.  Returns DDHDG_OK when converged, DDHDG_NOT_CONVERGED otherwise. */
+int ddhdg_newton(ddhdg_ctx *ctx, double *cell_state, double *trace_state,
+                 int thermo_eq, double abs_tol, double rel_tol, int max_it,
+                 double alpha, int *iterations, double *last_update_norm,
+                 ddhdg_stream_t stream);
+
+/* Per-stage device times (ms) of the last ddhdg_newton call. */
+int ddhdg_last_timings(const ddhdg_ctx *ctx, double *condense_ms,
+                       double *solve_ms, double *reconstruct_ms, int *steps);
+
+/* L2 projection of a scalar field given at cell and cell-face quadrature
+ * points into component comp of cell_state (scalar and weak-gradient
+ * displacement), as project_component (src/project_component.cpp:268-420) and
+ * compute_local_charge_neutrality_on_cells (src/thermodynamic_equilibrium.cpp:
+ * 47-213).  vals_cell [ncells][nqc], vals_face [ncells][2*dim][nqf]. */
+int ddhdg_project_cell(ddhdg_ctx *ctx, const double *vals_cell,
+                       const double *vals_face, int comp, double *cell_state,
+                       ddhdg_stream_t stream);
+/* L2 projection of face-point values [nfaces][nqf] onto the trace of comp. */
+int ddhdg_project_trace(ddhdg_ctx *ctx, const double *vals_face, int comp,
+                        double *trace_state, ddhdg_stream_t stream);
+/* project_component(phi_c, qf) (src/project_component.cpp:575-654) followed
+ * by project_cell_function_on_trace(l2_average) (src/copy_on_trace.cpp):
+ * density of comp (1: n, 2: p) from the quasi Fermi potential qf and the
+ * current V, projected on cells and averaged onto the trace. */
+int ddhdg_project_density(ddhdg_ctx *ctx, int comp, double qf,
+                          double *cell_state, double *trace_state,
+                          ddhdg_stream_t stream);
+
+/* Reference coordinates in [0,1]^dim of the quadrature points and support
+ * points the kernels use for a (dim, degree) pair, so that callers evaluate
+ * coefficient and boundary tables at exactly those points:
+ *   qref_c   [nqc][3]          QGauss(k+1) cell points (x fastest)
+ *   qref_f   [2*dim][nqf][3]   face points of local face f (axis f/2,
+ *                              side f%2; tangential axes (a+1)%d, (a+2)%d)
+ *   support  [k+1]             Gauss-Lobatto support points on [0,1]
+ * Any output pointer may be NULL. */
+int ddhdg_reference_points(int dim, int degree, double *qref_c, double *qref_f,
+                           double *support);
+
+/* Last error message of the calling thread (static storage). */
+const char *ddhdg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DDHDG_B200_H */
