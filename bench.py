@@ -1,0 +1,326 @@
+"""Benchmark of the per-Newton-step HDG hot path on B200.
+
+Workload: 2D p-n diode, 256 x 256 quads, HDG degree 2 (65 536 cells), GaAs
+material, SRH recombination, FP64.  A step is one pass of the hot path over
+all cells: the per-cell assembly + static condensation onto the trace
+(ddhdg_assemble_condense) and the cell reconstruction from a trace update
+(ddhdg_reconstruct).  The metric is HDG cells condensed per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank runs an independent replica of the diode
+(the hot path is per cell and per device; no data-path collective) and the
+time is the maximum over ranks.  --impl reference times the reference's
+algorithm on the host cores (the CPU oracle restating it; the reference
+itself needs deal.II and cannot be built here).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(dim=2, m=256, k=2)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def bytes_per_cell(dim, k, ncomp=3):
+    nb = (k + 1) ** dim
+    nf = (k + 1) ** (dim - 1)
+    F = 2 * dim
+    Nc_all = 3 * (dim + 1) * nb
+    Nt = F * ncomp * nf
+    Ns = ncomp * nb
+    condense = 8 * (Nc_all + F * 3 * nf + nb) + 8 * (Nt * Nt + 2 * Nt) + 4 * Nt + 8 * Ns * (1 + Nt)
+    reconstruct = 8 * (Ns * (1 + Nt) + Nc_all + 2 * F * 3 * nf) + 8 * Nc_all
+    return condense, reconstruct
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(k_sample_cells=4096, steps=1):
+    """The oracle (the reference's per-cell algorithm restated in C++,
+    OpenMP over cells) on a 64 x 64 slab of the same diode (same cell size,
+    degree and physics): assembly + condensation + reconstruction."""
+    from oracle.oracle import OracleSolver
+    from ddhdg_b200 import workloads as cases
+
+    m_side = int(round(k_sample_cells ** 0.5))
+    length = m_side / WORKLOAD["m"]
+    pb, prm, adim = cases.diode(dim=WORKLOAD["dim"], m=m_side, k=WORKLOAD["k"], length=length)
+    o = OracleSolver(pb, prm, adim, nthreads=os.cpu_count() or 1)
+    o.compute_local_charge_neutrality()
+    o.project_quasi_fermi(1)
+    o.project_quasi_fermi(2)
+    upd = 1e-6 * np.ones((o.nfaces, 3, o.nf))
+    best = None
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        o.assemble_condense()
+        o.reconstruct(upd)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return {"value": o.ncells / best, "unit": "cells/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": f"{m_side}x{m_side} cells of the 256x256 k=2 diode (same cell size), "
+                      f"assembly+condensation+reconstruction, {o.ncells} cells per step"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = []
+    info = None
+    for _ in range(args.warmup):
+        cpu_baseline(steps=1)
+    for _ in range(args.steps):
+        info = cpu_baseline(steps=1)
+        steps.append(info["value"])
+    v = float(np.median(steps))
+    line = {
+        "impl": "reference", "metric": "HDG cells condensed/s (assemble+condense+reconstruct)",
+        "value": v, "unit": "cells/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 65536 / v * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "2D p-n diode 256x256 quads, HDG degree 2, FP64 (bounded host sample)",
+                   "cells": 65536},
+        "cpu_baseline": dict(info, value=v),
+        "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+
+    from ddhdg_b200 import build as _b
+
+    _b.build()
+    from ddhdg_b200.solver import NPSolver
+    from ddhdg_b200 import _lib
+    from ddhdg_b200 import workloads as cases
+
+    pb, prm, adim = cases.diode(dim=WORKLOAD["dim"], m=WORKLOAD["m"], k=WORKLOAD["k"])
+    g = NPSolver(pb, prm, adim, device=str(dev))
+    g.compute_local_charge_neutrality()
+    for c in (1, 2):
+        _lib.check(g.L.ddhdg_project_density(g._ctx, c, 0.0, g.cell_state.data_ptr(),
+                                             g.trace_state.data_ptr(), g._sp()), "project_density")
+    torch.cuda.synchronize()
+    s = g.sizes()
+    nc, Nt = g.ncells, s.Nt
+    stream = g.stream
+    tt = torch.empty(nc * Nt * Nt, dtype=torch.float64, device=dev)
+    rhs = torch.empty(nc * Nt, dtype=torch.float64, device=dev)
+    dflag = torch.empty(nc * Nt, dtype=torch.int32, device=dev)
+    dval = torch.empty(nc * Nt, dtype=torch.float64, device=dev)
+    dtrace = (1e-6 * torch.ones(g.nfaces * 3 * g.nf, dtype=torch.float64, device=dev))
+    dcell = torch.empty(nc * g.Nc_all, dtype=torch.float64, device=dev)
+    L = g.L
+    sp = g._sp()
+
+    def condense():
+        _lib.check(L.ddhdg_assemble_condense(g._ctx, g.cell_state.data_ptr(), g.trace_state.data_ptr(), 0,
+                                             tt.data_ptr(), rhs.data_ptr(), dflag.data_ptr(), dval.data_ptr(),
+                                             sp), "condense")
+
+    def reconstruct():
+        _lib.check(L.ddhdg_reconstruct(g._ctx, g.cell_state.data_ptr(), g.trace_state.data_ptr(),
+                                       dtrace.data_ptr(), dcell.data_ptr(), 0, sp), "reconstruct")
+
+    for _ in range(max(args.warmup, 3)):
+        condense()
+        reconstruct()
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing (inputs in HBM; per-step traffic > L2)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps + 2)]
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    ev[0].record(stream)
+    for i in range(args.steps):
+        ev[1 + 3 * i].record(stream)
+        condense()
+        ev[2 + 3 * i].record(stream)
+        reconstruct()
+        ev[3 + 3 * i].record(stream)
+    ev[-1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = ev[0].elapsed_time(ev[-1])
+    cond_ms = [ev[1 + 3 * i].elapsed_time(ev[2 + 3 * i]) for i in range(args.steps)]
+    rec_ms = [ev[2 + 3 * i].elapsed_time(ev[3 + 3 * i]) for i in range(args.steps)]
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * nc / (ms_per_step * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers
+    pin_cell = torch.empty(nc * g.Nc_all, dtype=torch.float64).pin_memory()
+    pin_trace = torch.empty(g.nfaces * 3 * g.nf, dtype=torch.float64).pin_memory()
+    pin_dtrace = torch.empty(g.nfaces * 3 * g.nf, dtype=torch.float64).pin_memory()
+    pin_out = torch.empty(nc * g.Nc_all, dtype=torch.float64).pin_memory()
+    pin_cell.copy_(g.cell_state.cpu())
+    pin_trace.copy_(g.trace_state.cpu())
+    pin_dtrace.copy_(dtrace.cpu())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h2d = (pin_cell.numel() + pin_trace.numel() + pin_dtrace.numel()) * 8
+    d2h = pin_out.numel() * 8
+
+    def e2e_step():
+        g.cell_state.copy_(pin_cell, non_blocking=True)
+        g.trace_state.copy_(pin_trace, non_blocking=True)
+        dtrace.copy_(pin_dtrace, non_blocking=True)
+        condense()
+        reconstruct()
+        pin_out.copy_(dcell, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t2 = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t2.item()) / args.steps
+    e2e_value = world * nc / (e2e_ms * 1e-3)
+
+    if rank == 0:
+        hbm_peak, peak_kind = peaks()
+        bc, br = bytes_per_cell(WORKLOAD["dim"], WORKLOAD["k"])
+        cond_avg = float(np.mean(cond_ms))
+        achieved = bc * nc / (cond_avg * 1e-3) / 1e9
+        line = {
+            "metric": "HDG cells condensed/s (assemble+condense+reconstruct)",
+            "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "2D p-n diode 256x256 quads, HDG degree 2, FP64, plain method",
+                       "cells": nc, "trace_dofs_per_cell": Nt,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "per-step traffic (>1.2 GB) exceeds the 126 MB L2"},
+            "stages_ms": {"condense": cond_avg, "reconstruct": float(np.mean(rec_ms))},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": None,
+                         "kernel": "condense_kernel<2,2>", "peak_source": peak_kind,
+                         "algorithmic_bytes_per_cell": bc},
+            "e2e": {"value": e2e_value, "unit": "cells/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
