@@ -1615,6 +1615,44 @@ extern "C"
     return 0;
   }
 
+  // The local systems of every cell before the Schur complement (OpenMP).
+  // With update_trace != null the reconstruction-pass cc and cc_rhs are
+  // returned (ct, tc, tt, tt_rhs untouched).
+  int
+  oracle_local_cell_systems(const OrProblem *P, const double *cell_state,
+                            const double *trace_state, const double *update_trace,
+                            int thermo, double *cc, double *ct, double *tc,
+                            double *tt, double *cc_rhs, double *tt_rhs, int nthreads)
+  {
+    Oracle     o(*P);
+    const long ncells = o.G.ncells;
+    const long Nc = o.Nc, Nt = o.Nt;
+#ifdef _OPENMP
+    if (nthreads > 0)
+      omp_set_num_threads(nthreads);
+#pragma omp parallel
+#endif
+    {
+      Workspace w;
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+      for (long c = 0; c < ncells; ++c)
+        {
+          Outputs out{};
+          out.cc     = cc + c * Nc * Nc;
+          out.ct     = ct + c * Nc * Nt;
+          out.tc     = tc + c * Nt * Nc;
+          out.tt     = tt + c * Nt * Nt;
+          out.cc_rhs = cc_rhs + c * Nc;
+          out.tt_rhs = tt_rhs + c * Nt;
+          o.cell_system(c, cell_state, trace_state, update_trace,
+                        update_trace != nullptr, thermo != 0, false, w, out);
+        }
+    }
+    return 0;
+  }
+
   // Condensation pass over all cells: per-cell Schur complement tt [ncells][Nt][Nt],
   // rhs [ncells][Nt], Dirichlet flags/values [ncells][Nt].
   int

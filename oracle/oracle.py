@@ -63,6 +63,7 @@ def lib():
         L.oracle_tables.argtypes = [P] + [dp] * 8
         L.oracle_local_cell_system.argtypes = [P, dp, dp, ctypes.c_long, ctypes.c_int] + [dp] * 6
         L.oracle_assemble_condense.argtypes = [P, dp, dp, ctypes.c_int, dp, dp, ip, dp, ctypes.c_int]
+        L.oracle_local_cell_systems.argtypes = [P, dp, dp, dp, ctypes.c_int] + [dp] * 6 + [ctypes.c_int]
         L.oracle_reconstruct.argtypes = [P, dp, dp, dp, ctypes.c_int, dp, ctypes.c_int]
         L.oracle_srh.argtypes = [ctypes.c_double] * 6 + [dp] * 3
         L.oracle_srh_intrinsic.argtypes = [ctypes.c_double] * 5
@@ -376,6 +377,51 @@ class OracleSolver:
         lib().oracle_local_cell_system(ctypes.byref(P), _dp(cs), _dp(ts), int(cell), int(thermo),
                                        _dp(cc), _dp(ct), _dp(tc), _dp(tt), _dp(crhs), _dp(trhs))
         return dict(cc=cc, ct=ct, tc=tc, tt=tt, c=crhs, t=trhs)
+
+    def local_cell_systems(self, thermo=False, update_trace=None):
+        """Local systems (cc, ct, tc, tt, cc_rhs, tt_rhs) of every cell, as
+        assembled term by term before the Schur complement."""
+        P = self._struct(thermo=thermo)
+        sizes = np.zeros(9, dtype=np.int32)
+        lib().oracle_sizes(ctypes.byref(P), _ip(sizes))
+        Nc, Nt, n = int(sizes[1]), int(sizes[2]), self.ncells
+        cc = np.zeros((n, Nc, Nc))
+        ct = np.zeros((n, Nc, Nt))
+        tc = np.zeros((n, Nt, Nc))
+        tt = np.zeros((n, Nt, Nt))
+        cr = np.zeros((n, Nc))
+        tr = np.zeros((n, Nt))
+        cs = np.ascontiguousarray(self.cell_state)
+        ts = np.ascontiguousarray(self.trace_state)
+        ut = None if update_trace is None else np.ascontiguousarray(update_trace, dtype=np.float64)
+        lib().oracle_local_cell_systems(ctypes.byref(P), _dp(cs), _dp(ts),
+                                        None if ut is None else _dp(ut), int(thermo), _dp(cc), _dp(ct),
+                                        _dp(tc), _dp(tt), _dp(cr), _dp(tr), self.nthreads)
+        return cc, ct, tc, tt, cr, tr
+
+    def reconstruct_accurate(self, update_trace, thermo=False):
+        """Reconstruction-pass local systems solved with a row-equilibrated LU."""
+        cc, _, _, _, cr, _ = self.local_cell_systems(thermo, update_trace)
+        d = 1.0 / np.abs(cc).max(2, keepdims=True)
+        x = np.linalg.solve(cc * d, (cr * d[:, :, 0])[:, :, None])[:, :, 0]
+        P = self._struct(thermo=thermo)
+        out = np.zeros((self.ncells, self.Nc_all))
+        en = [True, False, False] if thermo else self.enabled
+        idx = [i for i in range(self.Nc_all) if en[i // ((self.dim + 1) * self.nb)]]
+        out[:, idx] = x
+        return out
+
+    def condense_accurate(self, thermo=False):
+        """Schur complement tt + tc cc^-1 [ct | cc_rhs] of the term-by-term
+        local systems with a row-equilibrated LU solve (numpy), used to
+        separate round-off of the reference's inversion from assembly."""
+        cc, ct, tc, tt, cr, tr = self.local_cell_systems(thermo)
+        d = 1.0 / np.abs(cc).max(2, keepdims=True)
+        rhs = np.concatenate([cr[:, :, None], ct], 2)
+        X = np.linalg.solve(cc * d, rhs * d)
+        S = tt + tc @ X[:, :, 1:]
+        g = tr + np.einsum("cij,cj->ci", tc, X[:, :, 0])
+        return S, g
 
     def assemble_condense(self, thermo=False):
         P = self._struct(thermo=thermo)

@@ -19,6 +19,14 @@ def make_pair(pb, prm, adim, seed=0, perturb=1e-3, thermo_start=True, enabled=(T
     rng = np.random.default_rng(seed)
     scale = np.maximum(np.abs(o.cell_state).max(0, keepdims=True), 1e-3)
     o.cell_state += perturb * scale * rng.standard_normal(o.cell_state.shape)
+    if thermo_start:
+        # keep the carrier densities positive: near n + p = 0 the SRH
+        # denominator cancels and amplifies round-off of any implementation
+        d, nb = o.dim, o.nb
+        for c in (1, 2):
+            blk = o.cell_block(c)
+            blk[:, d] = np.abs(blk[:, d]) + 1e-6
+            o.trace_state[:, c] = np.abs(o.trace_state[:, c]) + 1e-6
     o.trace_state += perturb * rng.standard_normal(o.trace_state.shape) * \
         np.maximum(np.abs(o.trace_state).max(), 1e-3)
     g = NPSolver(pb, prm, adim)
@@ -27,8 +35,8 @@ def make_pair(pb, prm, adim, seed=0, perturb=1e-3, thermo_start=True, enabled=(T
     return g, o
 
 
-def rel_err(a, b):
+def rel_err(a, b, floor=1e-300):
     a = np.asarray(a)
     b = np.asarray(b)
-    scale = max(np.abs(b).max(), 1e-300)
+    scale = max(np.abs(b).max(), floor)
     return float(np.abs(a - b).max() / scale)

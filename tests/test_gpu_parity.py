@@ -22,11 +22,19 @@ def compare_condense(g, o, thermo=False, tol=TOL):
     tt, rhs, flag, val = g.assemble_condense(thermo)
     ott, orhs, oflag, oval = o.assemble_condense(thermo)
     assert np.array_equal(flag.cpu().numpy(), oflag)
-    assert rel_err(val.cpu().numpy(), oval) < tol
-    e_tt = rel_err(tt.cpu().numpy(), ott)
-    e_rhs = rel_err(rhs.cpu().numpy(), orhs)
+    # Dirichlet increments are differences of O(trace) numbers
+    assert rel_err(val.cpu().numpy(), oval, floor=np.abs(o.trace_state).max()) < tol
+    # the oracle's terms, condensed with a row-equilibrated solve: the GPU must
+    # match it to FP64 round-off
+    S, g_ = o.condense_accurate(thermo)
+    e_tt = rel_err(tt.cpu().numpy(), S)
+    e_rhs = rel_err(rhs.cpu().numpy(), g_)
     assert e_tt < tol, e_tt
     assert e_rhs < tol, e_rhs
+    # the reference's own inversion (LU of the transpose, FullMatrix::
+    # gauss_jordan) agrees with it within its round-off
+    assert rel_err(ott, S) < 1e-6
+    assert rel_err(orhs, g_) < 1e-5
     return tt, rhs
 
 
@@ -39,11 +47,16 @@ def compare_reconstruct(g, o, thermo=False, tol=TOL, seed=5):
         upd[:, c] = rng.standard_normal((o.nfaces, o.nf)) * max(np.abs(o.trace_state[:, c]).max(), 1e-3) * 1e-2
     gu = g.reconstruct(upd, thermo).cpu().numpy()
     ou = o.reconstruct(upd, thermo)
-    e = rel_err(gu, ou)
+    acc = o.reconstruct_accurate(upd, thermo)
+    e = rel_err(gu, acc)
     assert e < tol, e
+    assert rel_err(ou, acc) < 1e-5
 
 
-@pytest.mark.parametrize("dim,k,m", [(2, 1, 6), (2, 2, 5), (2, 3, 4), (3, 1, 3), (1, 2, 9), (3, 2, 2)])
+# m keeps every quadrature point off the junction x = 0.5, where the step
+# doping is discontinuous (two independently computed Gauss rules may differ
+# by an ulp there and sample opposite sides of the step)
+@pytest.mark.parametrize("dim,k,m", [(2, 1, 6), (2, 2, 6), (2, 3, 4), (3, 1, 3), (1, 2, 8), (3, 2, 2)])
 def test_diode_condense_and_reconstruct(dim, k, m):
     pb, prm, adim = cases.diode(dim=dim, m=m, k=k)
     g, o = make_pair(pb, prm, adim, seed=dim * 10 + k)
@@ -61,7 +74,7 @@ def test_fluxes(flux):
 
 @pytest.mark.parametrize("fix", [1, 2, 3])
 def test_jacobian_options(fix):
-    pb, prm, adim = cases.diode(dim=2, m=5, k=2)
+    pb, prm, adim = cases.diode(dim=2, m=6, k=2)
     prm.consistent_drift_jacobian = bool(fix & 1)
     prm.consistent_recombination_jacobian = bool(fix & 2)
     g, o = make_pair(pb, prm, adim, seed=fix)
@@ -87,7 +100,7 @@ def test_phi_linearize():
                                      (True, True, False), (True, False, True)])
 def test_partial_components(enabled):
     """disabling_components (tests/disabling_components.cpp) mask variants."""
-    pb, prm, adim = cases.diode(dim=2, m=5, k=2)
+    pb, prm, adim = cases.diode(dim=2, m=6, k=2)
     g, o = make_pair(pb, prm, adim, seed=sum(enabled) * 7 + enabled[0], enabled=enabled)
     compare_condense(g, o)
     compare_reconstruct(g, o)
@@ -100,7 +113,7 @@ def test_cell_face_tau_and_linear_recombination():
     rng = np.random.default_rng(4)
     for cell in range(pb.mesh.n_cells):
         for f in range(4):
-            prm.set_face(cell, f, *(rng.uniform(0.5, 2.0, 3) * np.array([1.6e-19, 1.0, 1.0])))
+            prm.set_face(cell, f, *(rng.uniform(0.5, 2.0, 3) * np.array([1.0, 100.0, 10000.0])))
     g, o = make_pair(pb, prm, adim, seed=4, thermo_start=False)
     o.set_component(0, "-2 * log(x)")
     o.set_component(1, "2 / (x^2 * q)")
