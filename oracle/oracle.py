@@ -419,8 +419,12 @@ class OracleSolver:
         d = 1.0 / np.abs(cc).max(2, keepdims=True)
         rhs = np.concatenate([cr[:, :, None], ct], 2)
         X = np.linalg.solve(cc * d, rhs * d)
-        S = tt + tc @ X[:, :, 1:]
-        g = tr + np.einsum("cij,cj->ci", tc, X[:, :, 0])
+        tcX = tc @ X
+        S = tt + tcX[:, :, 1:]
+        g = tr + tcX[:, :, 0]
+        # magnitude of the summed terms (round-off scale of S and g)
+        self.condense_term_scale = (max(np.abs(tt).max(), np.abs(tcX[:, :, 1:]).max()),
+                                    max(np.abs(tr).max(), np.abs(tcX[:, :, 0]).max()))
         return S, g
 
     def assemble_condense(self, thermo=False):

@@ -1,8 +1,13 @@
 """Parity of the CUDA hot path against the CPU oracle (the reference's
-algorithm restated), through the C ABI.  Tolerances are relative to the
-largest entry of each compared array; the CUDA path eliminates the flux
-unknowns before factorising, so agreement is to FP64 round-off amplified by
-the local condition number, stated per test."""
+algorithm restated), through the C ABI.
+
+The condensed systems are compared with the oracle's term-by-term local
+matrices condensed by a row-equilibrated LU.  The tolerance 1e-10 is relative
+to the magnitude of the terms that are summed: in the junction cells of the
+diodes the condensed right-hand side is a difference of two terms up to 5e6
+times larger than itself, so FP64 round-off of any implementation is relative
+to those terms, not to the result.  The oracle's own reference-style inversion
+is pinned against the same quantity separately."""
 
 import numpy as np
 import pytest
@@ -27,14 +32,15 @@ def compare_condense(g, o, thermo=False, tol=TOL):
     # the oracle's terms, condensed with a row-equilibrated solve: the GPU must
     # match it to FP64 round-off
     S, g_ = o.condense_accurate(thermo)
-    e_tt = rel_err(tt.cpu().numpy(), S)
-    e_rhs = rel_err(rhs.cpu().numpy(), g_)
+    s_tt, s_rhs = o.condense_term_scale
+    e_tt = rel_err(tt.cpu().numpy(), S, floor=s_tt)
+    e_rhs = rel_err(rhs.cpu().numpy(), g_, floor=s_rhs)
     assert e_tt < tol, e_tt
     assert e_rhs < tol, e_rhs
     # the reference's own inversion (LU of the transpose, FullMatrix::
     # gauss_jordan) agrees with it within its round-off
-    assert rel_err(ott, S) < 1e-6
-    assert rel_err(orhs, g_) < 1e-5
+    assert rel_err(ott, S, floor=s_tt) < tol
+    assert rel_err(orhs, g_, floor=s_rhs) < tol
     return tt, rhs
 
 
