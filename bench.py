@@ -168,6 +168,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells-per-side", type=int, default=WORKLOAD["m"],
+                    help="smaller meshes of the same diode for profiling runs")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -193,7 +195,9 @@ def main():
     from ddhdg_b200 import _lib
     from ddhdg_b200 import workloads as cases
 
-    pb, prm, adim = cases.diode(dim=WORKLOAD["dim"], m=WORKLOAD["m"], k=WORKLOAD["k"])
+    m_side = args.cells_per_side
+    pb, prm, adim = cases.diode(dim=WORKLOAD["dim"], m=m_side, k=WORKLOAD["k"],
+                                length=m_side / WORKLOAD["m"])
     g = NPSolver(pb, prm, adim, device=str(dev))
     g.compute_local_charge_neutrality()
     for c in (1, 2):
@@ -300,7 +304,7 @@ def main():
             "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "2D p-n diode 256x256 quads, HDG degree 2, FP64, plain method",
+            "config": {"workload": f"2D p-n diode {m_side}x{m_side} quads (cell size 1/256 um), HDG degree 2, FP64, plain method",
                        "cells": nc, "trace_dofs_per_cell": Nt,
                        "parallelism": f"replicas x{world}",
                        "l2": "per-step traffic (>1.2 GB) exceeds the 126 MB L2"},
