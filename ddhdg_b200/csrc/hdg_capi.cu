@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/ddhdg_b200.h"
+#include "hdg_condense.cuh"
 #include "hdg_kernels.cuh"
 #include "hdg_tables.h"
 
@@ -457,7 +458,7 @@ namespace
   void
   pick(CondenseFn &cf, ReconstructFn &rf)
   {
-    cf = condense_kernel<D, K>;
+    cf = condense2_kernel<D, K>;
     rf = reconstruct_kernel<D, K>;
   }
 
@@ -478,21 +479,18 @@ namespace
       }
   }
 
-  // warps per block, chunk size and table staging so that the workspace fits
-  // in the 227 KB of shared memory of a CTA
+  // chunk size and table staging so that one cell's workspace (one CTA of
+  // CondenseTPB threads) fits in the 227 KB of shared memory of a CTA
   int
-  launch_shape(const ddhdg_ctx *c, const Mode &m, int &wpb, int &chunk, int &stage,
-               size_t &smem)
+  launch_shape(const ddhdg_ctx *c, const Mode &m, int &chunk, int &stage, size_t &smem)
   {
     const size_t limit = 220 * 1024;
-    chunk              = 8;
-    const WsOff  w     = ws_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, chunk);
-    const size_t ws    = (size_t)w.total * sizeof(double);
     const size_t tb    = (((size_t)c->to.total + 1) & ~(size_t)1) * sizeof(double);
     for (stage = 1; stage >= 0; --stage)
-      for (wpb = 8; wpb >= 1; wpb /= 2)
+      for (chunk = 16; chunk >= 1; chunk /= 2)
         {
-          smem = (stage ? tb : 0) + (size_t)wpb * ws;
+          const Ws2Off w = ws2_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, chunk);
+          smem           = (stage ? tb : 0) + (size_t)w.total * sizeof(double);
           if (smem <= limit)
             return DDHDG_OK;
         }
@@ -908,6 +906,13 @@ ddhdg_ctx_create(const ddhdg_problem_desc *d, ddhdg_ctx **out)
     c->to.P      = put(c->T.P);
     c->to.Q      = put(c->T.Q);
     c->to.minv   = put(c->T.minv);
+    c->to.TLc    = put(c->T.TLc);
+    c->to.TLg    = put(c->T.TLg);
+    c->to.TLf    = put(c->T.TLf);
+    c->to.RTk    = put(c->T.RTk);
+    c->to.RTr    = put(c->T.RTr);
+    c->to.RQk    = put(c->T.RQk);
+    c->to.RQr    = put(c->T.RQr);
     c->to.total  = (int)blob.size();
     int r        = c->tables.upload(blob.data(), blob.size());
     if (r)
@@ -1036,21 +1041,20 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
   P.dflag       = dflag;
   P.dval        = dval;
   P.ycache      = m.ycache.p;
-  int    wpb, chunk, stage;
+  int    chunk, stage;
   size_t smem;
-  if ((r = launch_shape(c, m, wpb, chunk, stage, smem)))
+  if ((r = launch_shape(c, m, chunk, stage, smem)))
     return r;
-  P.wpb   = wpb;
+  P.wpb   = 1;
   P.chunk = chunk;
   P.stage = stage;
   CK(cudaFuncSetAttribute(cf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, wpb * 32, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, CondenseTPB, smem));
   if (per_sm < 1)
     return fail(DDHDG_BAD_ARG, "condense kernel does not fit on an SM");
-  const int64_t blocks_needed = (c->ncells + wpb - 1) / wpb;
-  const int     grid = (int)std::min<int64_t>(blocks_needed, (int64_t)per_sm * c->sm_count);
-  cf<<<grid, wpb * 32, smem, (cudaStream_t)stream>>>(P);
+  const int grid = (int)std::min<int64_t>(c->ncells, (int64_t)per_sm * c->sm_count);
+  cf<<<grid, CondenseTPB, smem, (cudaStream_t)stream>>>(P);
   CK(cudaGetLastError());
   return DDHDG_OK;
 }

@@ -39,6 +39,14 @@ namespace ddhdg
     std::vector<double> PW_f;   // [nb][F][nqf]   normal component
     std::vector<double> QW_c;   // [F*nf][nqc][dim]
     std::vector<double> QW_f;   // [F*nf][F][nqf] normal component
+    // channel tables of the condensation kernel (contraction index first)
+    std::vector<double> TLc;  // [nqc][nb]        w_q phi_a(q)
+    std::vector<double> TLg;  // [nqc*dim][nb]    w_q d_s phi_a(q)
+    std::vector<double> TLf;  // [F*nqf][nb]      w_fq phi_a(fq)
+    std::vector<double> RTk;  // [nqc*dim][nb]    PW_e(q, s)
+    std::vector<double> RTr;  // [F*nqf][nb]      PWf_e(fq)
+    std::vector<double> RQk;  // [nqc*dim][F*nf]  QW_t(q, s)
+    std::vector<double> RQr;  // [F*nqf][F*nf]    QWf_t(fq)
     std::vector<double> qref_c; // [nqc][3] reference coordinates
     std::vector<double> qref_f; // [F][nqf][3]
     std::vector<double> gl;     // [k+1] support points
@@ -436,6 +444,40 @@ namespace ddhdg
               }
           }
       }
+    const int Fq = F * nqf, Ft = F * nf;
+    T.TLc.assign(nqc * nb, 0.);
+    T.TLg.assign(nqc * D * nb, 0.);
+    T.TLf.assign(Fq * nb, 0.);
+    T.RTk.assign(nqc * D * nb, 0.);
+    T.RTr.assign(Fq * nb, 0.);
+    T.RQk.assign(nqc * D * Ft, 0.);
+    T.RQr.assign(Fq * Ft, 0.);
+    for (int q = 0; q < nqc; ++q)
+      for (int a = 0; a < nb; ++a)
+        {
+          T.TLc[q * nb + a] = T.w_c[q] * T.phi_c[q * nb + a];
+          for (int s = 0; s < D; ++s)
+            {
+              T.TLg[(q * D + s) * nb + a] = T.w_c[q] * T.grad_c[(q * nb + a) * D + s];
+              T.RTk[(q * D + s) * nb + a] = T.PW_c[(a * nqc + q) * D + s];
+            }
+        }
+    for (int q = 0; q < nqc; ++q)
+      for (int s = 0; s < D; ++s)
+        for (int t = 0; t < Ft; ++t)
+          T.RQk[(q * D + s) * Ft + t] = T.QW_c[(t * nqc + q) * D + s];
+    for (int f = 0; f < F; ++f)
+      for (int qf = 0; qf < nqf; ++qf)
+        {
+          const int fq = f * nqf + qf;
+          for (int a = 0; a < nb; ++a)
+            {
+              T.TLf[fq * nb + a] = T.w_f[fq] * T.phi_f[fq * nb + a];
+              T.RTr[fq * nb + a] = T.PW_f[(a * F + f) * nqf + qf];
+            }
+          for (int t = 0; t < Ft; ++t)
+            T.RQr[fq * Ft + t] = T.QW_f[(t * F + f) * nqf + qf];
+        }
     return T;
   }
 } // namespace ddhdg
