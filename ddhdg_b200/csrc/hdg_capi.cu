@@ -21,6 +21,7 @@
 
 #include "../../include/ddhdg_b200.h"
 #include "hdg_condense.cuh"
+#include "hdg_condense3.cuh"
 #include "hdg_kernels.cuh"
 #include "hdg_tables.h"
 
@@ -105,6 +106,7 @@ namespace
     DevBuf<int32_t>       rowptr, colind;
     DevBuf<uint8_t>       slots; // [ncells][F][F]
     DevBuf<double>        ycache, tt, rhs, dval, csr, grhs, x, dtrace, dcell;
+    DevBuf<double>        rscratch; // per-CTA R blocks of the condense kernel, if needed
     DevBuf<int32_t>       dflag;
     std::vector<int32_t>  perm; // nested-dissection order of the trace dofs
     DevBuf<int32_t>       d_perm, d_iperm, prow, pcol;
@@ -458,7 +460,12 @@ namespace
   void
   pick(CondenseFn &cf, ReconstructFn &rf)
   {
-    cf = condense2_kernel<D, K>;
+    // warp-per-cell register kernel when one lane can own one row of the
+    // scalar system, CTA-per-cell shared-memory kernel otherwise
+    if constexpr (3 * Dims<D, K>::nb <= 32)
+      cf = condense3_kernel<D, K>;
+    else
+      cf = condense2_kernel<D, K>;
     rf = reconstruct_kernel<D, K>;
   }
 
@@ -479,21 +486,26 @@ namespace
       }
   }
 
-  // chunk size and table staging so that one cell's workspace (one CTA of
-  // CondenseTPB threads) fits in the 227 KB of shared memory of a CTA
+  // chunk size, table staging and placement of the right-hand-side block R
+  // so that one cell's workspace (one CTA of CondenseTPB threads) fits in
+  // the 227 KB of shared memory of a CTA; R moves to global memory only when
+  // nothing else makes it fit
   int
-  launch_shape(const ddhdg_ctx *c, const Mode &m, int &chunk, int &stage, size_t &smem)
+  launch_shape(const ddhdg_ctx *c, const Mode &m, int &chunk, int &stage, bool &r_global,
+               size_t &smem)
   {
     const size_t limit = 220 * 1024;
     const size_t tb    = (((size_t)c->to.total + 1) & ~(size_t)1) * sizeof(double);
-    for (stage = 1; stage >= 0; --stage)
-      for (chunk = 16; chunk >= 1; chunk /= 2)
-        {
-          const Ws2Off w = ws2_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, chunk);
-          smem           = (stage ? tb : 0) + (size_t)w.total * sizeof(double);
-          if (smem <= limit)
-            return DDHDG_OK;
-        }
+    for (int rg = 0; rg < 2; ++rg)
+      for (stage = 1; stage >= 0; --stage)
+        for (chunk = 16; chunk >= 1; chunk /= 2)
+          {
+            r_global       = rg != 0;
+            const Ws2Off w = ws2_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, chunk, r_global);
+            smem           = (stage ? tb : 0) + (size_t)w.total * sizeof(double);
+            if (smem <= limit)
+              return DDHDG_OK;
+          }
     return fail(DDHDG_BAD_ARG, "the per-cell workspace does not fit in shared memory");
   }
 
@@ -1041,20 +1053,52 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
   P.dflag       = dflag;
   P.dval        = dval;
   P.ycache      = m.ycache.p;
-  int    chunk, stage;
+  int    threads;
   size_t smem;
-  if ((r = launch_shape(c, m, chunk, stage, smem)))
-    return r;
-  P.wpb   = 1;
-  P.chunk = chunk;
-  P.stage = stage;
+  int64_t units;
+  if (3 * c->nb <= 32)
+    {
+      // warp per cell: as many warps per CTA as shared memory allows
+      const Ws3Off w   = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol);
+      const size_t per = (size_t)w.total * sizeof(double);
+      int          wpb = (int)std::min<size_t>(Condense3MaxWPB, (220 * 1024) / per);
+      if (wpb < 1)
+        return fail(DDHDG_BAD_ARG, "the per-cell workspace does not fit in shared memory");
+      P.wpb   = wpb;
+      P.stage = 0;
+      threads = wpb * 32;
+      smem    = (size_t)wpb * per;
+      units   = (c->ncells + wpb - 1) / wpb;
+    }
+  else
+    {
+      int  chunk, stage;
+      bool r_global;
+      if ((r = launch_shape(c, m, chunk, stage, r_global, smem)))
+        return r;
+      P.wpb   = 1;
+      P.chunk = chunk;
+      P.stage = stage;
+      threads = CondenseTPB;
+      units   = c->ncells;
+      if (r_global)
+        {
+          int per_sm = 0;
+          CK(cudaFuncSetAttribute(cf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, threads, smem));
+          const int64_t g = std::min<int64_t>(units, (int64_t)std::max(per_sm, 1) * c->sm_count);
+          if ((r = m.rscratch.alloc((size_t)g * c->nb * m.ncomp * m.ncol)))
+            return r;
+          P.rscratch = m.rscratch.p;
+        }
+    }
   CK(cudaFuncSetAttribute(cf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, CondenseTPB, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, threads, smem));
   if (per_sm < 1)
     return fail(DDHDG_BAD_ARG, "condense kernel does not fit on an SM");
-  const int grid = (int)std::min<int64_t>(c->ncells, (int64_t)per_sm * c->sm_count);
-  cf<<<grid, CondenseTPB, smem, (cudaStream_t)stream>>>(P);
+  const int grid = (int)std::min<int64_t>(units, (int64_t)per_sm * c->sm_count);
+  cf<<<grid, threads, smem, (cudaStream_t)stream>>>(P);
   CK(cudaGetLastError());
   return DDHDG_OK;
 }

@@ -37,11 +37,11 @@ namespace ddhdg
     int al, be, ka, ga, rh;             // per pair (9) coefficients
     int ctc, ctd, tcS, tcW, ttc, rhsf;  // per component / pair face data
     int r0, r1, rf;                     // residual coefficients
-    int S, R, Y, g, dfl, rhsA, Tr, lmul, total;
+    int S, R, g, dfl, rhsA, U, Wn, X, total;
   };
 
   __host__ __device__ inline Ws2Off
-  ws2_layout(int dim, int nb, int nf, int ncomp, int ncol, int chunk)
+  ws2_layout(int dim, int nb, int nf, int ncomp, int ncol, int chunk, bool r_global = false)
   {
     const int F = 2 * dim, nqc = nb, Fq = F * nf;
     const int Ns = ncomp * nb, Nt = F * ncomp * nf;
@@ -79,19 +79,19 @@ namespace ddhdg
     o.r1    = take(3 * nqc * dim);
     o.rf    = take(3 * Fq);
     o.S     = take(Ns * (Ns + 1));
-    o.R     = take(Ns * ncol);
-    o.Y     = take(Ns * ncol);
-    o.lmul  = take(Ns);
+    o.R     = r_global ? 0 : take(Ns * ncol); // else a slice of KParams::rscratch
     o.g     = take(Nt);
     o.dfl   = take(Nt);
-    o.rhsA  = take(Nt > Ns ? Nt : Ns);
-    o.Tr    = take(Nt * Ns);
+    o.rhsA  = take(Nt);
+    o.U     = take(chunk * 3 * Fq);
+    o.Wn    = take(chunk * 3 * Fq);
+    o.X     = take(Nt * chunk);
     o.total = p;
     return o;
   }
 
   template <int DIM, int K>
-  __global__ void __launch_bounds__(CondenseTPB, 4)
+  __global__ void __launch_bounds__(CondenseTPB)
   condense2_kernel(const KParams P)
   {
     using Dm          = Dims<DIM, K>;
@@ -105,11 +105,9 @@ namespace ddhdg
     constexpr int NCA = Dm::Nc_all;
     constexpr int T   = CondenseTPB;
     constexpr int NW  = T / 32;
-    constexpr int NSMAX = 3 * nb; // largest scalar system (all components)
     extern __shared__ double smem[];
+    __shared__ int sh_piv;
     __shared__ int sh_sing;
-    __shared__ int piv_s[NSMAX];
-    __shared__ int used_s[NSMAX];
 
     const int tid   = threadIdx.x;
     const int lane  = tid & 31;
@@ -119,6 +117,7 @@ namespace ddhdg
     const int Nt    = F * ncomp * nf;
     const int ncol  = P.ncol;
     const int ldS   = Ns + 1;
+    const int CH    = P.chunk;
     const bool two  = ncol > 1 + Nt;
 
     // ---- constant tables, staged once per CTA
@@ -147,7 +146,7 @@ namespace ddhdg
     const double *QW_c   = tb + P.to.QW_c;
     const double *QW_f   = tb + P.to.QW_f;
 
-    const Ws2Off wo = ws2_layout(DIM, nb, nf, ncomp, ncol, 1);
+    const Ws2Off wo = ws2_layout(DIM, nb, nf, ncomp, ncol, CH, P.rscratch != nullptr);
     double *ws = smem + (P.stage ? ((P.to.total + 1) & ~1) : 0);
     double *coef = ws + wo.coef, *lam = ws + wo.lam, *c0 = ws + wo.c0, *W0 = ws + wo.W0,
            *qc = ws + wo.qc, *c0f = ws + wo.c0f, *W0n = ws + wo.W0n, *tr0 = ws + wo.tr0,
@@ -156,9 +155,12 @@ namespace ddhdg
            *rh = ws + wo.rh, *ctc = ws + wo.ctc, *ctd = ws + wo.ctd, *tcS = ws + wo.tcS,
            *tcW = ws + wo.tcW, *ttc = ws + wo.ttc, *rhsf = ws + wo.rhsf, *r0 = ws + wo.r0,
            *r1 = ws + wo.r1, *rf = ws + wo.rf, *S = ws + wo.S, *R = ws + wo.R,
-           *gv = ws + wo.g, *dfl = ws + wo.dfl, *rhsA = ws + wo.rhsA, *Tr = ws + wo.Tr,
-           *Yb = ws + wo.Y, *lmul = ws + wo.lmul;
-    double *const R_base = R, *const Y_base = Yb;
+           *gv = ws + wo.g, *dfl = ws + wo.dfl, *rhsA = ws + wo.rhsA, *Ub = ws + wo.U,
+           *Wb = ws + wo.Wn, *Xc = ws + wo.X;
+    // R of the largest systems (3D k = 2 with drift columns: 210 KB) lives
+    // in this CTA's slice of a global buffer, which stays in L2
+    if (P.rscratch)
+      R = P.rscratch + (int64_t)blockIdx.x * Ns * ncol;
 
     const double eps = P.eps, mun = P.mun, mup = P.mup, U_T = P.U_T;
     const bool   thermo   = P.thermo != 0;
@@ -172,8 +174,6 @@ namespace ddhdg
 
     for (int64_t cell = blockIdx.x; cell < P.ncells; cell += gridDim.x)
       {
-        R  = R_base;
-        Yb = Y_base;
         // ------------------------------------------------------ state
         const double *cs = P.cell_state + cell * NCA;
         for (int i = tid; i < NCA; i += T)
@@ -633,7 +633,7 @@ namespace ddhdg
           sh_sing = 0;
         __syncthreads();
 
-        // ------------------------------ equilibrate the rows of [S | R]
+        // -------------------------- equilibrate rows, LU with partial pivoting
         for (int i = warp; i < Ns; i += NW)
           {
             double mx = 0.;
@@ -649,32 +649,21 @@ namespace ddhdg
               R[i * ncol + c] *= sc;
           }
         __syncthreads();
-
-        // -------- Gauss-Jordan elimination of [S | R] with partial pivoting
-        // Column j is eliminated from every other row; pivot rows are chosen
-        // among the rows not used yet (virtual pivoting, no row swaps).
-        // Afterwards row piv_s[j] of R divided by S[piv_s[j]][j] is row j of
-        // Y = S^-1 R.  Columns already eliminated are neither read nor
-        // written again, so every step is one barrier-separated update.
-        if (tid < Ns)
-          used_s[tid] = 0;
-        __syncthreads();
         for (int j = 0; j < Ns; ++j)
           {
             if (warp == 0)
               {
                 double best = -1.;
-                int    bi   = Ns;
-                for (int i = lane; i < Ns; i += 32)
-                  if (!used_s[i])
-                    {
-                      const double v = fabs(S[i * ldS + j]);
-                      if (v > best || (v == best && i < bi))
-                        {
-                          best = v;
-                          bi   = i;
-                        }
-                    }
+                int    bi   = j;
+                for (int i = j + lane; i < Ns; i += 32)
+                  {
+                    const double v = fabs(S[i * ldS + j]);
+                    if (v > best)
+                      {
+                        best = v;
+                        bi   = i;
+                      }
+                  }
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1)
                   {
@@ -686,57 +675,57 @@ namespace ddhdg
                         bi   = oi;
                       }
                   }
-                if (!(best > 0.) || !isfinite(best) || bi >= Ns)
-                  {
-                    bi = (bi >= Ns) ? 0 : bi;
-                    if (lane == 0)
-                      sh_sing = 1;
-                  }
-                const double pv  = S[bi * ldS + j];
-                const double inv = (pv != 0.) ? 1. / pv : 0.;
-                for (int i = lane; i < Ns; i += 32)
-                  lmul[i] = (i == bi) ? 0. : S[i * ldS + j] * inv;
                 if (lane == 0)
                   {
-                    piv_s[j]   = bi;
-                    used_s[bi] = 1;
+                    sh_piv = bi;
+                    if (!(best > 0.) || !isfinite(best))
+                      sh_sing = 1;
                   }
               }
             __syncthreads();
-            const int p    = piv_s[j];
-            const int wS   = Ns - j - 1;      // S columns j+1 .. Ns-1
-            const int wtot = wS + ncol;
-            for (int i = warp; i < Ns; i += NW)
+            const int p = sh_piv;
+            if (p != j)
               {
-                const double l = lmul[i];
-                if (l == 0.)
-                  continue;
-                for (int c = lane; c < wtot; c += 32)
+                for (int c = tid; c < Ns + ncol; c += T)
                   {
-                    if (c < wS)
-                      S[i * ldS + j + 1 + c] -= l * S[p * ldS + j + 1 + c];
-                    else
-                      R[i * ncol + c - wS] -= l * R[p * ncol + c - wS];
+                    double *x  = (c < Ns) ? &S[j * ldS + c] : &R[j * ncol + c - Ns];
+                    double *y  = (c < Ns) ? &S[p * ldS + c] : &R[p * ncol + c - Ns];
+                    const double t0 = *x;
+                    *x              = *y;
+                    *y              = t0;
                   }
+                __syncthreads();
+              }
+            const double piv = S[j * ldS + j];
+            const double inv = (piv != 0.) ? 1. / piv : 0.;
+            for (int i = j + 1 + warp; i < Ns; i += NW)
+              {
+                const double l = S[i * ldS + j] * inv;
+                for (int c = j + 1 + lane; c < Ns; c += 32)
+                  S[i * ldS + c] -= l * S[j * ldS + c];
+                for (int c = lane; c < ncol; c += 32)
+                  R[i * ncol + c] -= l * R[j * ncol + c];
+              }
+            __syncthreads();
+          }
+        // back substitution: R becomes Y
+        for (int j = Ns - 1; j >= 0; --j)
+          {
+            const double piv = S[j * ldS + j];
+            const double inv = (piv != 0.) ? 1. / piv : 0.;
+            for (int c = tid; c < ncol; c += T)
+              R[j * ncol + c] *= inv;
+            __syncthreads();
+            for (int i = warp; i < j; i += NW)
+              {
+                const double u = S[i * ldS + j];
+                for (int c = lane; c < ncol; c += 32)
+                  R[i * ncol + c] -= u * R[j * ncol + c];
               }
             __syncthreads();
           }
         if (tid == 0 && sh_sing)
           atomicExch(P.status, 3);
-        // Y rows: Y[j] = R[piv[j]] / S[piv[j]][j], gathered into Ybuf
-        for (int idx = tid; idx < Ns * ncol; idx += T)
-          {
-            const int    j = idx / ncol, c = idx % ncol;
-            const int    p = piv_s[j];
-            const double d = S[p * ldS + j];
-            Yb[idx]        = (d != 0.) ? R[p * ncol + c] / d : 0.;
-          }
-        __syncthreads();
-        {
-          double *tmp = R;
-          R           = Yb;
-          Yb          = tmp;
-        }
 
         // ------------------------ keep Y for the reconstruction [col][row]
         {
@@ -745,117 +734,122 @@ namespace ddhdg
             yc[idx] = R[(idx % Ns) * ncol + idx / Ns];
         }
 
-        // ---------- reduced trace operator T = tc_c + tc_W P on the faces
-        for (int idx = tid; idx < Nt * Ns; idx += T)
+        // --------------------------- condensation on the faces, by chunks
+        for (int i = tid; i < Nt; i += T)
+          rhsA[i] = 0.;
+        double *tt_out = P.tt + cell * (int64_t)Nt * Nt;
+        for (int cbeg = 0; cbeg < 1 + Nt; cbeg += CH)
           {
-            const int i = idx / Ns, j = idx % Ns;
-            const int fi = i / (ncomp * nf), ci = (i / nf) % ncomp, mi = i % nf;
-            const int cj = j / nb, e = j % nb;
-            const int b  = P.comps[ci];
-            const int pr = b * 3 + P.comps[cj];
-            double    v  = 0.;
-#pragma unroll
-            for (int qf = 0; qf < nqf; ++qf)
+            const int nch = min(CH, 1 + Nt - cbeg);
+            // scalar value and normal flux of every column on the faces
+            for (int idx = tid; idx < nch * ncomp * Fq; idx += T)
               {
-                const int fq = fi * nqf + qf;
-                double    z  = tcW[pr * Fq + fq] * RTr[fq * nb + e];
-                if (cj == ci)
-                  z += tcS[b * Fq + fq] * phi_f[fq * nb + e];
-                v += w_f[fq] * xi[qf * nf + mi] * z;
+                const int cc = idx / (ncomp * Fq);
+                const int r_ = idx % (ncomp * Fq);
+                const int ce = r_ / Fq, fq = r_ % Fq;
+                const int col = cbeg + cc;
+                double    u = 0., wn;
+                if (col == 0)
+                  wn = Wrf[ce * Fq + fq];
+                else
+                  {
+                    const int t = col - 1;
+                    const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
+                    wn = (ct == ce) ? RQr[fq * Ft + ft * nf + mt] : 0.;
+                  }
+                const bool add = two && col > 0;
+#pragma unroll
+                for (int e = 0; e < nb; ++e)
+                  {
+                    double y = R[(ce * nb + e) * ncol + col];
+                    if (add)
+                      y += R[(ce * nb + e) * ncol + col + Nt];
+                    u += phi_f[fq * nb + e] * y;
+                    wn += RTr[fq * nb + e] * y;
+                  }
+                Ub[(cc * 3 + ce) * Fq + fq] = u;
+                Wb[(cc * 3 + ce) * Fq + fq] = wn;
               }
-            Tr[i * Ns + j] = v;
-          }
-        // combined residual column (Dirichlet columns folded in, in order)
-        for (int j = tid; j < Ns; j += T)
-          {
-            double acc = R[j * ncol];
-            for (int t = 0; t < Nt; ++t)
-              if (dfl[t] != 0.)
-                {
-                  double y = R[j * ncol + 1 + t];
-                  if (two)
-                    y += R[j * ncol + 1 + Nt + t];
-                  acc -= gv[t] * y;
-                }
-            rhsA[j] = acc;
-          }
-        __syncthreads();
-
-        // --------- tt = tt_face + T Y_t + tc_W Q_t, coalesced along t
-        {
-          double   *tt_out = P.tt + cell * (int64_t)Nt * Nt;
-          const int RG     = T / Nt > 0 ? T / Nt : 1; // row groups
-          const int rows   = (Nt + RG - 1) / RG;
-          for (int idx = tid; idx < Nt * RG; idx += T)
-            {
-              const int t  = idx % Nt;
-              const int rg = idx / Nt;
-              const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
-              const int tq = ft * nf + mt;
-              const bool colD = dfl[t] != 0.;
-              for (int i = rg * rows; i < min(Nt, (rg + 1) * rows); ++i)
-                {
-                  double o = 0.;
-                  if (!colD && dfl[i] == 0.)
-                    {
-                      const int fi = i / (ncomp * nf), ci = (i / nf) % ncomp, mi = i % nf;
-                      const int b  = P.comps[ci];
-                      double    x  = 0.;
-                      for (int j = 0; j < Ns; ++j)
-                        {
-                          double y = R[j * ncol + 1 + t];
-                          if (two)
-                            y += R[j * ncol + 1 + Nt + t];
-                          x += Tr[i * Ns + j] * y;
-                        }
-                      // flux part of the trace column itself (tc_W Q_t)
-                      const int pr = b * 3 + P.comps[ct];
+            __syncthreads();
+            // combined trace-equation integrand -> Ub
+            for (int idx = tid; idx < nch * ncomp * Fq; idx += T)
+              {
+                const int cc = idx / (ncomp * Fq);
+                const int r_ = idx % (ncomp * Fq);
+                const int ce = r_ / Fq, fq = r_ % Fq;
+                const int b  = P.comps[ce];
+                double    v  = tcS[b * Fq + fq] * Ub[(cc * 3 + ce) * Fq + fq];
+                for (int cp = 0; cp < ncomp; ++cp)
+                  v += tcW[(b * 3 + P.comps[cp]) * Fq + fq] * Wb[(cc * 3 + cp) * Fq + fq];
+                Ub[(cc * 3 + ce) * Fq + fq] = v;
+              }
+            __syncthreads();
+            // tc X for every trace row and column of the chunk
+            for (int idx = tid; idx < Nt * nch; idx += T)
+              {
+                const int i = idx / nch, cc = idx % nch;
+                const int fi = i / (ncomp * nf), ci = (i / nf) % ncomp, mi = i % nf;
+                const int col = cbeg + cc;
+                double    x   = 0.;
 #pragma unroll
-                      for (int qf = 0; qf < nqf; ++qf)
-                        {
-                          const int fq = fi * nqf + qf;
-                          x += w_f[fq] * xi[qf * nf + mi] * tcW[pr * Fq + fq] * RQr[fq * Ft + tq];
-                        }
-                      // face part of tt (same face and component)
-                      if (ft == fi && ct == ci)
+                for (int qf = 0; qf < nqf; ++qf)
+                  x += w_f[fi * nqf + qf] * xi[qf * nf + mi] *
+                       Ub[(cc * 3 + ci) * Fq + fi * nqf + qf];
+                const bool rowD = dfl[i] != 0.;
+                Xc[i * CH + cc] = x;
+                if (col > 0)
+                  {
+                    const int t = col - 1;
+                    double    o = 0.;
+                    if (dfl[t] == 0. && !rowD)
+                      {
+                        o              = x;
+                        const int ft   = t / (ncomp * nf);
+                        const int ct   = (t / nf) % ncomp;
+                        if (ft == fi && ct == ci)
+                          {
+                            const int b  = P.comps[ci];
+                            const int mt = t % nf;
 #pragma unroll
-                        for (int qf = 0; qf < nqf; ++qf)
-                          x += w_f[fi * nqf + qf] * ttc[b * Fq + fi * nqf + qf] *
-                               xi[qf * nf + mi] * xi[qf * nf + mt];
-                      o = x;
-                    }
-                  tt_out[(int64_t)i * Nt + t] = o;
-                }
-            }
-        }
+                            for (int qf = 0; qf < nqf; ++qf)
+                              o += w_f[fi * nqf + qf] * ttc[b * Fq + fi * nqf + qf] *
+                                   xi[qf * nf + mi] * xi[qf * nf + mt];
+                          }
+                      }
+                    tt_out[(int64_t)i * Nt + t] = o;
+                  }
+              }
+            __syncthreads();
+            // residual column and Dirichlet columns -> rhs, in column order
+            for (int i = tid; i < Nt; i += T)
+              {
+                double acc = rhsA[i];
+                for (int cc = 0; cc < nch; ++cc)
+                  {
+                    const int col = cbeg + cc;
+                    if (col == 0)
+                      acc += Xc[i * CH + cc];
+                    else if (dfl[col - 1] != 0.)
+                      acc -= Xc[i * CH + cc] * gv[col - 1];
+                  }
+                rhsA[i] = acc;
+              }
+            __syncthreads();
+          }
 
         // ------------------------------------- right-hand side and flags
         for (int i = tid; i < Nt; i += T)
           {
-            const int  fi = i / (ncomp * nf), ci = (i / nf) % ncomp, mi = i % nf;
-            const int  b  = P.comps[ci];
+            const int fi = i / (ncomp * nf), ci = (i / nf) % ncomp, mi = i % nf;
+            const int b  = P.comps[ci];
             const bool rowD = dfl[i] != 0.;
             double     r    = 0.;
             if (!rowD)
               {
-                for (int j = 0; j < Ns; ++j)
-                  r += Tr[i * Ns + j] * rhsA[j];
 #pragma unroll
                 for (int qf = 0; qf < nqf; ++qf)
-                  {
-                    const int fq = fi * nqf + qf;
-                    double    z  = rhsf[b * Fq + fq];
-                    // flux residual (column 0 base) and the Dirichlet columns' flux
-                    for (int cp = 0; cp < ncomp; ++cp)
-                      z += tcW[(b * 3 + P.comps[cp]) * Fq + fq] * Wrf[cp * Fq + fq];
-                    for (int t = 0; t < Nt; ++t)
-                      if (dfl[t] != 0.)
-                        {
-                          const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
-                          z -= gv[t] * tcW[(b * 3 + P.comps[ct]) * Fq + fq] * RQr[fq * Ft + ft * nf + mt];
-                        }
-                    r += w_f[fq] * xi[qf * nf + mi] * z;
-                  }
+                  r += w_f[fi * nqf + qf] * xi[qf * nf + mi] * rhsf[b * Fq + fi * nqf + qf];
+                r += rhsA[i];
               }
             P.rhs[cell * Nt + i]   = r;
             P.dflag[cell * Nt + i] = rowD ? 1 : 0;

@@ -1,0 +1,923 @@
+// Per-cell assembly + static condensation, one warp per cell (sm_100a, FP64),
+// for local scalar systems of at most 32 unknowns (3 (k+1)^d <= 32: 2D k <= 2,
+// 3D k = 1, 1D).
+//
+// Same mathematics as condense2_kernel (hdg_condense.cuh): the flux unknowns
+// are eliminated through the constant mass matrix and the scalar system
+// S y = R of the enabled components is solved for the residual and for every
+// trace dof.  The difference is the execution model: every lane owns one row
+// of the local system in registers, the Gauss-Jordan inverse of S runs with
+// warp shuffles (virtual partial pivoting, no barriers), and the products
+// Y = S^-1 R and tt = T Y are formed with per-lane register accumulators, so
+// that each lane has tens of independent FMAs in flight.  Warps are
+// independent; the constant tables are read through the L1 cache.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "hdg_condense.cuh"
+
+namespace ddhdg
+{
+  constexpr int Condense3MaxWPB = 8; // warps (cells) per CTA at most
+
+  struct Ws3Off
+  {
+    int coef, lam, c0, W0, qc, c0f, W0n, tr0, Wrc, Wrf, tau, bcs;
+    int al, be, ka, ga, rh, ctc, ctd, tcS, tcW, ttc, rhsf, r0, r1, rf;
+    int R, g, dfl, Yc, total;
+  };
+
+  __host__ __device__ inline Ws3Off
+  ws3_layout(int dim, int nb, int nf, int ncomp, int ncol)
+  {
+    const int F = 2 * dim, nqc = nb, Fq = F * nf;
+    const int Ns = ncomp * nb, Nt = F * ncomp * nf;
+    Ws3Off    o;
+    int       p = 0;
+    auto      take = [&p](int n) {
+      const int r = p;
+      p += (n + 1) & ~1;
+      return r;
+    };
+    o.coef  = take(3 * (dim + 1) * nb);
+    o.lam   = take(F * 3 * nf);
+    o.c0    = take(3 * nqc);
+    o.W0    = take(3 * dim * nqc);
+    o.qc    = take(6 * nqc);
+    o.c0f   = take(3 * Fq);
+    o.W0n   = take(3 * Fq);
+    o.tr0   = take(3 * Fq);
+    o.Wrc   = take(3 * dim * nqc);
+    o.Wrf   = take(3 * Fq);
+    o.tau   = take(F * 3);
+    o.bcs   = take(F * 3);
+    o.al    = take(9 * nqc);
+    o.be    = take(9 * nqc * dim);
+    o.ka    = take(9 * nqc);
+    o.ga    = take(9 * Fq);
+    o.rh    = take(9 * Fq);
+    o.ctc   = take(3 * Fq);
+    o.ctd   = take(3 * Fq);
+    o.tcS   = take(3 * Fq);
+    o.tcW   = take(9 * Fq);
+    o.ttc   = take(3 * Fq);
+    o.rhsf  = take(3 * Fq);
+    o.r0    = take(3 * nqc);
+    o.r1    = take(3 * nqc * dim);
+    o.rf    = take(3 * Fq);
+    o.R     = take(Ns * ncol);
+    o.g     = take(Nt);
+    o.dfl   = take(Nt);
+    o.Yc    = take(Ns);
+    o.total = p;
+    return o;
+  }
+
+  template <int DIM, int K>
+  __global__ void __launch_bounds__(Condense3MaxWPB * 32, 1)
+  condense3_kernel(const KParams P)
+  {
+    using Dm            = Dims<DIM, K>;
+    constexpr int nb    = Dm::nb;
+    constexpr int nf    = Dm::nf;
+    constexpr int nqc   = Dm::nqc;
+    constexpr int nqf   = Dm::nqf;
+    constexpr int F     = Dm::F;
+    constexpr int Fq    = F * nqf;
+    constexpr int Ft    = F * nf;
+    constexpr int NCA   = Dm::Nc_all;
+    constexpr int NSMAX = 3 * nb;
+    static_assert(NSMAX <= 32, "one lane per row of the scalar system");
+    extern __shared__ double smem[];
+    __shared__ int piv3[Condense3MaxWPB][NSMAX];
+
+    const int  lane  = threadIdx.x & 31;
+    const int  warp  = threadIdx.x >> 5;
+    const int  ncomp = P.ncomp;
+    const int  Ns    = ncomp * nb;
+    const int  Nt    = F * ncomp * nf;
+    const int  ncol  = P.ncol;
+    const bool two   = ncol > 1 + Nt;
+
+    const double *tb = P.tables;
+    const double *phi_c  = tb + P.to.phi_c;
+    const double *w_f    = tb + P.to.w_f;
+    const double *xi     = tb + P.to.xi;
+    const double *fminvw = tb + P.to.fminvw;
+    const double *phi_f  = tb + P.to.phi_f;
+    const double *TLc    = tb + P.to.TLc;
+    const double *TLg    = tb + P.to.TLg;
+    const double *TLf    = tb + P.to.TLf;
+    const double *RTk    = tb + P.to.RTk;
+    const double *RTr    = tb + P.to.RTr;
+    const double *RQk    = tb + P.to.RQk;
+    const double *RQr    = tb + P.to.RQr;
+    const double *PW_c   = tb + P.to.PW_c;
+    const double *PW_f   = tb + P.to.PW_f;
+    const double *QW_c   = tb + P.to.QW_c;
+    const double *QW_f   = tb + P.to.QW_f;
+
+    const Ws3Off wo = ws3_layout(DIM, nb, nf, ncomp, ncol);
+    double      *ws = smem + warp * wo.total;
+    double *coef = ws + wo.coef, *lam = ws + wo.lam, *c0 = ws + wo.c0, *W0 = ws + wo.W0,
+           *qc = ws + wo.qc, *c0f = ws + wo.c0f, *W0n = ws + wo.W0n, *tr0 = ws + wo.tr0,
+           *Wrc = ws + wo.Wrc, *Wrf = ws + wo.Wrf, *taus = ws + wo.tau, *bcs = ws + wo.bcs,
+           *al = ws + wo.al, *be = ws + wo.be, *ka = ws + wo.ka, *ga = ws + wo.ga,
+           *rh = ws + wo.rh, *ctc = ws + wo.ctc, *ctd = ws + wo.ctd, *tcS = ws + wo.tcS,
+           *tcW = ws + wo.tcW, *ttc = ws + wo.ttc, *rhsf = ws + wo.rhsf, *r0 = ws + wo.r0,
+           *r1 = ws + wo.r1, *rf = ws + wo.rf, *R = ws + wo.R,
+           *gv = ws + wo.g, *dfl = ws + wo.dfl, *Yc = ws + wo.Yc;
+
+    const double eps = P.eps, mun = P.mun, mup = P.mup, U_T = P.U_T;
+    const bool   thermo   = P.thermo != 0;
+    const bool   phi_mode = thermo || P.phi_linearize;
+    const double ds       = (P.jfix & 1) ? -1. : 1.;
+    const int    flux     = P.flux;
+    int          cmp[3]   = {P.comps[0], P.comps[1], P.comps[2]};
+    bool         nen = false, pen = false;
+    for (int c = 0; c < ncomp; ++c)
+      {
+        nen |= cmp[c] == 1;
+        pen |= cmp[c] == 2;
+      }
+    const int wpb = blockDim.x >> 5;
+
+    for (int64_t cell = (int64_t)blockIdx.x * wpb + warp; cell < P.ncells;
+         cell += (int64_t)gridDim.x * wpb)
+      {
+        // keeps the table loads inside the cell loop (no hoisting of
+        // thousands of loop-invariant values into registers)
+        asm volatile("" ::: "memory");
+        // ------------------------------------------------------------ state
+        int64_t face_id[F];
+#pragma unroll
+        for (int f = 0; f < F; ++f)
+          face_id[f] = face_index(P, cell, f, DIM);
+        const double *cs = P.cell_state + cell * NCA;
+        for (int i = lane; i < NCA; i += 32)
+          coef[i] = cs[i];
+        for (int i = lane; i < F * 3 * nf; i += 32)
+          {
+            int64_t Fi = 0;
+#pragma unroll
+            for (int f = 0; f < F; ++f)
+              if (f == i / (3 * nf))
+                Fi = face_id[f];
+            lam[i] = P.trace_state[Fi * 3 * nf + (i % (3 * nf))];
+          }
+        if (lane < F * 3)
+          {
+            const int f = lane / 3, b = lane % 3;
+            int64_t   Fi = 0;
+#pragma unroll
+            for (int g = 0; g < F; ++g)
+              if (g == f)
+                Fi = face_id[g];
+            taus[lane] = P.tau_table ? P.tau_table[(cell * F + f) * 3 + b] : P.tau[b];
+            bcs[lane]  = (double)P.face_bc[Fi * 3 + b];
+          }
+        __syncwarp();
+
+        // ------------------------------------ fields at quadrature points
+        for (int i = lane; i < 3 * (DIM + 1) * nqc; i += 32)
+          {
+            const int     b  = i / ((DIM + 1) * nqc);
+            const int     s  = (i / nqc) % (DIM + 1);
+            const int     q  = i % nqc;
+            const double *cf = coef + (b * (DIM + 1) + s) * nb;
+            double        v  = 0.;
+#pragma unroll
+            for (int a = 0; a < nb; ++a)
+              v += phi_c[q * nb + a] * cf[a];
+            if (s < DIM)
+              W0[(b * DIM + s) * nqc + q] = v;
+            else
+              c0[b * nqc + q] = v;
+          }
+        for (int i = lane; i < 3 * Fq; i += 32)
+          {
+            const int     b  = i / Fq;
+            const int     fq = i % Fq;
+            const int     f  = fq / nqf, qf = fq % nqf;
+            const double  sg = (f & 1) ? 1. : -1.;
+            const double *ph = phi_f + fq * nb;
+            const double *cS = coef + (b * (DIM + 1) + DIM) * nb;
+            const double *cW = coef + (b * (DIM + 1) + f / 2) * nb;
+            double        u = 0., wn = 0., t = 0.;
+#pragma unroll
+            for (int a = 0; a < nb; ++a)
+              {
+                u += ph[a] * cS[a];
+                wn += ph[a] * cW[a];
+              }
+#pragma unroll
+            for (int m = 0; m < nf; ++m)
+              t += xi[qf * nf + m] * lam[(f * 3 + b) * nf + m];
+            c0f[i] = u;
+            W0n[i] = sg * wn;
+            tr0[i] = t;
+          }
+        __syncwarp();
+
+        // --------------------- point coefficients and the flux residual
+        for (int q = lane; q < nqc; q += 32)
+          {
+            const double n0 = c0[nqc + q], p0 = c0[2 * nqc + q], V0 = c0[q];
+            double       r = 0., drn = 0., drp = 0.;
+            if (nen || pen)
+              {
+                const double rf_ = P.n_rescale;
+                if (P.rec_type == 1)
+                  {
+                    const double ni  = P.srh_ni / rf_;
+                    const double num = n0 * p0 - ni * ni;
+                    const double den = P.srh_tau_p * (n0 + ni) + P.srh_tau_n * (p0 + ni);
+                    r                = num * rf_ / den;
+                    drn              = p0 / den - num * P.srh_tau_p / (den * den);
+                    drp              = n0 / den - num * P.srh_tau_n / (den * den);
+                  }
+                else
+                  {
+                    const int64_t idx = cell * nqc + q;
+                    const double  a_  = P.rec_a ? P.rec_a[idx] : 0.;
+                    const double  b_  = P.rec_b ? P.rec_b[idx] : 0.;
+                    const double  c_  = P.rec_c ? P.rec_c[idx] : 0.;
+                    r                 = a_ + (b_ * n0 + c_ * p0) * rf_;
+                    drn               = b_;
+                    drp               = c_;
+                  }
+                r /= P.rec_rescale;
+                drn /= P.rec_rescale;
+                drp /= P.rec_rescale;
+                if (P.jfix & 2)
+                  {
+                    drn *= rf_;
+                    drp *= rf_;
+                  }
+              }
+            double phider = 0., phirhs = 0.;
+            if (phi_mode)
+              {
+                const double KbT = KB_ * P.T / (Q_ * P.V_rescale);
+                const double evr = P.ev / (Q_ * P.V_rescale);
+                const double ecr = P.ec / (Q_ * P.V_rescale);
+                double       phn = 0., php = 0.;
+                if (!thermo)
+                  {
+                    const double U  = P.T * (KB_ / Q_);
+                    const double Vp = V0 * P.V_rescale;
+                    if (nen)
+                      phn = (Vp - P.ec / Q_ - U * log(n0 * P.n_rescale / P.nc)) / P.V_rescale;
+                    if (pen)
+                      php = (Vp - P.ev / Q_ + U * log(p0 * P.n_rescale / P.nv)) / P.V_rescale;
+                  }
+                const double e1 = exp((evr - V0 + php) / KbT);
+                const double e2 = exp((V0 - phn - ecr) / KbT);
+                phider          = -1. / P.n_rescale * (P.nv / KbT * e1 + P.nc / KbT * e2);
+                phirhs          = 1. / P.n_rescale * (P.nv * e1 - P.nc * e2);
+              }
+            qc[0 * nqc + q] = r;
+            qc[1 * nqc + q] = drn;
+            qc[2 * nqc + q] = drp;
+            qc[3 * nqc + q] = phider;
+            qc[4 * nqc + q] = phirhs;
+            qc[5 * nqc + q] = P.doping[cell * nqc + q];
+          }
+        for (int i = lane; i < ncomp * DIM * nqc; i += 32)
+          {
+            const int     ce = i / (DIM * nqc);
+            const int     b  = cmp[ce];
+            const int     s  = (i / nqc) % DIM;
+            const int     q  = i % nqc;
+            const double *cS = coef + (b * (DIM + 1) + DIM) * nb;
+            double        v  = -W0[(b * DIM + s) * nqc + q];
+#pragma unroll
+            for (int e = 0; e < nb; ++e)
+              v += PW_c[(e * nqc + q) * DIM + s] * cS[e];
+#pragma unroll
+            for (int t = 0; t < Ft; ++t)
+              v -= QW_c[(t * nqc + q) * DIM + s] * lam[((t / nf) * 3 + b) * nf + (t % nf)];
+            Wrc[(ce * DIM + s) * nqc + q] = v;
+          }
+        for (int i = lane; i < ncomp * Fq; i += 32)
+          {
+            const int     ce = i / Fq;
+            const int     b  = cmp[ce];
+            const int     fq = i % Fq;
+            const int     f = fq / nqf, qf = fq % nqf;
+            const double *cS = coef + (b * (DIM + 1) + DIM) * nb;
+            double        v  = -W0n[b * Fq + fq];
+#pragma unroll
+            for (int e = 0; e < nb; ++e)
+              v += PW_f[(e * F + f) * nqf + qf] * cS[e];
+#pragma unroll
+            for (int t = 0; t < Ft; ++t)
+              v -= QW_f[(t * F + f) * nqf + qf] * lam[((t / nf) * 3 + b) * nf + (t % nf)];
+            Wrf[ce * Fq + fq] = v;
+          }
+        __syncwarp();
+
+        // ------------------------------- channel coefficients per pair
+        for (int i = lane; i < 9 * nqc; i += 32)
+          {
+            const int    pr = i / nqc, q = i % nqc;
+            const int    b = pr / 3, bp = pr % 3;
+            const double n0 = c0[nqc + q], p0 = c0[2 * nqc + q];
+            double       a_ = 0., k_ = 0., bb[DIM];
+#pragma unroll
+            for (int s = 0; s < DIM; ++s)
+              bb[s] = 0.;
+            if (b == 0)
+              {
+                if (bp == 0)
+                  {
+                    a_ = phi_mode ? -qc[3 * nqc + q] : 0.;
+                    k_ = -eps;
+                  }
+                else if (!phi_mode)
+                  a_ = (bp == 1) ? 1. : -1.;
+              }
+            else
+              {
+                if (bp == 0)
+                  k_ = (b == 1) ? ds * n0 * mun : -ds * p0 * mup;
+                else
+                  {
+                    a_ = (bp == 1) ? -qc[nqc + q] : -qc[2 * nqc + q];
+                    if (bp == b)
+                      {
+                        k_              = U_T * ((b == 1) ? mun : mup);
+                        const double sg = (b == 1) ? -mun : mup;
+#pragma unroll
+                        for (int s = 0; s < DIM; ++s)
+                          bb[s] = sg * W0[s * nqc + q];
+                      }
+                  }
+              }
+            al[i] = a_;
+            ka[i] = k_;
+#pragma unroll
+            for (int s = 0; s < DIM; ++s)
+              be[i * DIM + s] = bb[s];
+          }
+        for (int i = lane; i < 9 * Fq; i += 32)
+          {
+            const int    pr = i / Fq, fq = i % Fq, f = fq / nqf;
+            const int    b = pr / 3, bp = pr % 3;
+            const double E0n = W0n[fq];
+            const bool   cellside = (flux == 0) || (flux == 2 && E0n > 0.);
+            double       g_ = 0., r_ = 0., w_ = 0.;
+            if (b == 0)
+              {
+                if (bp == 0)
+                  {
+                    g_ = taus[f * 3];
+                    r_ = eps;
+                    w_ = -eps;
+                  }
+              }
+            else
+              {
+                const double mu   = (b == 1) ? mun : mup;
+                const double sg   = (b == 1) ? 1. : -1.;
+                const double cstr = cellside ? c0f[b * Fq + fq] : tr0[b * Fq + fq];
+                if (bp == 0)
+                  {
+                    r_ = sg * mu * cstr;
+                    w_ = -sg * mu * cstr;
+                  }
+                else if (bp == b)
+                  {
+                    g_ = (cellside ? sg * mu * E0n : 0.) - taus[f * 3 + b];
+                    r_ = -U_T * mu;
+                    w_ = U_T * mu;
+                  }
+              }
+            ga[i]  = g_;
+            rh[i]  = r_;
+            tcW[i] = w_;
+          }
+        for (int i = lane; i < 3 * Fq; i += 32)
+          {
+            const int    b = i / Fq, fq = i % Fq, f = fq / nqf, qf = fq % nqf;
+            const double E0n = W0n[fq];
+            const bool   cellside = (flux == 0) || (flux == 2 && E0n > 0.);
+            const bool   drift    = (flux == 1) || (flux == 2 && E0n <= 0.);
+            const double tb_ = taus[f * 3 + b];
+            const double cb0 = c0f[b * Fq + fq], tb0 = tr0[b * Fq + fq];
+            double       c_, d_ = 0., s_, t_, rr;
+            if (b == 0)
+              {
+                c_ = -tb_;
+                s_ = -tb_;
+                t_ = -tb_;
+                rr = -eps * E0n - tb_ * cb0 + tb_ * tb0;
+              }
+            else
+              {
+                const double mu   = (b == 1) ? mun : mup;
+                const double sg   = (b == 1) ? 1. : -1.;
+                const double cstr = cellside ? cb0 : tb0;
+                c_                = tb_;
+                d_                = drift ? sg * mu * E0n : 0.;
+                s_                = (cellside ? -sg * mu * E0n : 0.) + tb_;
+                t_                = tb_ + d_;
+                rr = -sg * cstr * mu * E0n + U_T * mu * W0n[b * Fq + fq] + tb_ * cb0 - tb_ * tb0;
+              }
+            if (bcs[f * 3 + b] == 2. && !thermo)
+              {
+                int64_t Fi = 0;
+#pragma unroll
+                for (int g = 0; g < F; ++g)
+                  if (g == f)
+                    Fi = face_id[g];
+                rr += P.face_bc_val[(Fi * 3 + b) * nqf + qf];
+              }
+            ctc[i]  = c_;
+            ctd[i]  = d_;
+            tcS[i]  = s_;
+            ttc[i]  = t_;
+            rhsf[i] = rr;
+          }
+        __syncwarp();
+
+        // ------------------------------------------ residual coefficients
+        for (int i = lane; i < ncomp * nqc; i += 32)
+          {
+            const int    ce = i / nqc, q = i % nqc, b = cmp[ce];
+            const double n0 = c0[nqc + q], p0 = c0[2 * nqc + q];
+            double       v0, v1[DIM];
+            if (b == 0)
+              {
+                v0 = qc[5 * nqc + q] + (phi_mode ? qc[4 * nqc + q] : (p0 - n0));
+#pragma unroll
+                for (int s = 0; s < DIM; ++s)
+                  v1[s] = eps * W0[s * nqc + q];
+              }
+            else
+              {
+                const double mu = (b == 1) ? mun : mup;
+                const double cb = (b == 1) ? n0 : -p0;
+                v0              = qc[q];
+#pragma unroll
+                for (int s = 0; s < DIM; ++s)
+                  v1[s] = cb * mu * W0[s * nqc + q] - U_T * mu * W0[(b * DIM + s) * nqc + q];
+              }
+            for (int cp = 0; cp < ncomp; ++cp)
+              {
+                const double k_ = ka[(b * 3 + cmp[cp]) * nqc + q];
+#pragma unroll
+                for (int s = 0; s < DIM; ++s)
+                  v1[s] -= k_ * Wrc[(cp * DIM + s) * nqc + q];
+              }
+            r0[ce * nqc + q] = v0;
+#pragma unroll
+            for (int s = 0; s < DIM; ++s)
+              r1[(ce * nqc + q) * DIM + s] = v1[s];
+          }
+        for (int i = lane; i < ncomp * Fq; i += 32)
+          {
+            const int    ce = i / Fq, fq = i % Fq, b = cmp[ce];
+            const double E0n = W0n[fq];
+            const bool   cellside = (flux == 0) || (flux == 2 && E0n > 0.);
+            const double tb_ = taus[(fq / nqf) * 3 + b];
+            const double cb0 = c0f[b * Fq + fq], tb0 = tr0[b * Fq + fq];
+            double       v;
+            if (b == 0)
+              v = tb_ * tb0 - eps * E0n - tb_ * cb0;
+            else
+              {
+                const double mu   = (b == 1) ? mun : mup;
+                const double sg   = (b == 1) ? 1. : -1.;
+                const double cstr = cellside ? cb0 : tb0;
+                const double Jf   = sg * cstr * mu * E0n - U_T * mu * W0n[b * Fq + fq];
+                v                 = -tb_ * tb0 - Jf + tb_ * cb0;
+              }
+            for (int cp = 0; cp < ncomp; ++cp)
+              v -= rh[(b * 3 + cmp[cp]) * Fq + fq] * Wrf[cp * Fq + fq];
+            rf[ce * Fq + fq] = v;
+          }
+        for (int t = lane; t < Nt; t += 32)
+          {
+            const int f = t / (ncomp * nf), ce = (t / nf) % ncomp, m = t % nf;
+            const int b = cmp[ce];
+            double    g = 0., fl = 0.;
+            if (bcs[f * 3 + b] == 1.)
+              {
+                fl = 1.;
+                if (!thermo)
+                  {
+                    int64_t Fi = 0;
+#pragma unroll
+                    for (int gg = 0; gg < F; ++gg)
+                      if (gg == f)
+                        Fi = face_id[gg];
+#pragma unroll
+                    for (int qf = 0; qf < nqf; ++qf)
+                      g += fminvw[m * nqf + qf] *
+                           (P.face_bc_val[(Fi * 3 + b) * nqf + qf] - tr0[(b * F + f) * nqf + qf]);
+                  }
+              }
+            gv[t]  = g;
+            dfl[t] = fl;
+          }
+        __syncwarp();
+
+        // ---------------- right-hand sides R, one row per lane -> smem
+        const bool act = lane < Ns;
+        const int  ci  = act ? lane / nb : 0;
+        const int  a   = act ? lane % nb : 0;
+        const int  bi  = cmp[ci];
+        if (act)
+          {
+            // residual column
+            {
+              const double *r0p = r0 + ci * nqc;
+              const double *r1p = r1 + ci * nqc * DIM;
+              const double *rfp = rf + ci * Fq;
+              double        v   = 0.;
+#pragma unroll
+              for (int q = 0; q < nqc; ++q)
+                {
+                  v += TLc[q * nb + a] * r0p[q];
+#pragma unroll
+                  for (int s = 0; s < DIM; ++s)
+                    v += TLg[(q * DIM + s) * nb + a] * r1p[q * DIM + s];
+                }
+#pragma unroll
+              for (int fq = 0; fq < Fq; ++fq)
+                v += TLf[fq * nb + a] * rfp[fq];
+              R[lane * ncol] = v;
+            }
+            // trace columns, one trial component at a time
+            for (int cj = 0; cj < ncomp; ++cj)
+              {
+                const int     pr  = bi * 3 + cmp[cj];
+                const double *kap = ka + pr * nqc;
+                const double *rhp = rh + pr * Fq;
+                double        acc[Ft];
+#pragma unroll
+                for (int t = 0; t < Ft; ++t)
+                  acc[t] = 0.;
+#pragma unroll 1
+                for (int q = 0; q < nqc; ++q)
+                  {
+                    const double kq = kap[q];
+#pragma unroll
+                    for (int s = 0; s < DIM; ++s)
+                      {
+                        const double w = kq * TLg[(q * DIM + s) * nb + a];
+#pragma unroll
+                        for (int t = 0; t < Ft; ++t)
+                          acc[t] -= w * RQk[(q * DIM + s) * Ft + t];
+                      }
+                  }
+#pragma unroll 1
+                for (int fq = 0; fq < Fq; ++fq)
+                  {
+                    const double w = rhp[fq] * TLf[fq * nb + a];
+#pragma unroll
+                    for (int t = 0; t < Ft; ++t)
+                      acc[t] -= w * RQr[fq * Ft + t];
+                  }
+                if (cj == ci)
+                  {
+#pragma unroll
+                    for (int f = 0; f < F; ++f)
+#pragma unroll
+                      for (int qf = 0; qf < nqf; ++qf)
+                        {
+                          const int    fq = f * nqf + qf;
+                          const double w  = ctc[bi * Fq + fq] * TLf[fq * nb + a];
+#pragma unroll
+                          for (int m = 0; m < nf; ++m)
+                            acc[f * nf + m] += w * xi[qf * nf + m];
+                        }
+                  }
+#pragma unroll
+                for (int f = 0; f < F; ++f)
+#pragma unroll
+                  for (int m = 0; m < nf; ++m)
+                    R[lane * ncol + 1 + (f * ncomp + cj) * nf + m] = acc[f * nf + m];
+                if (two)
+                  {
+#pragma unroll
+                    for (int f = 0; f < F; ++f)
+#pragma unroll
+                      for (int m = 0; m < nf; ++m)
+                        {
+                          double d = 0.;
+                          if (cj == ci)
+#pragma unroll
+                            for (int qf = 0; qf < nqf; ++qf)
+                              {
+                                const int fq = f * nqf + qf;
+                                d += ctd[bi * Fq + fq] * TLf[fq * nb + a] * xi[qf * nf + m];
+                              }
+                          R[lane * ncol + 1 + Nt + (f * ncomp + cj) * nf + m] = d;
+                        }
+                  }
+              }
+          }
+
+        // ------------ S row per lane, in-place Gauss-Jordan inverse
+        double srow[NSMAX];
+#pragma unroll
+        for (int j = 0; j < NSMAX; ++j)
+          srow[j] = 0.;
+        if (act)
+          {
+#pragma unroll
+            for (int cj = 0; cj < 3; ++cj)
+              {
+                if (cj >= ncomp)
+                  break;
+                const int     pr  = bi * 3 + cmp[cj];
+                const double *alp = al + pr * nqc;
+                const double *kap = ka + pr * nqc;
+                const double *bep = be + pr * nqc * DIM;
+                const double *gap = ga + pr * Fq;
+                const double *rhp = rh + pr * Fq;
+                double        acc[nb];
+#pragma unroll
+                for (int e = 0; e < nb; ++e)
+                  acc[e] = 0.;
+#pragma unroll 1
+                for (int q = 0; q < nqc; ++q)
+                  {
+                    double lt = alp[q] * TLc[q * nb + a];
+                    double kt[DIM];
+#pragma unroll
+                    for (int s = 0; s < DIM; ++s)
+                      {
+                        const double tg = TLg[(q * DIM + s) * nb + a];
+                        lt += bep[q * DIM + s] * tg;
+                        kt[s] = kap[q] * tg;
+                      }
+#pragma unroll
+                    for (int e = 0; e < nb; ++e)
+                      {
+                        double v = lt * phi_c[q * nb + e];
+#pragma unroll
+                        for (int s = 0; s < DIM; ++s)
+                          v += kt[s] * RTk[(q * DIM + s) * nb + e];
+                        acc[e] += v;
+                      }
+                  }
+#pragma unroll 1
+                for (int fq = 0; fq < Fq; ++fq)
+                  {
+                    const double tf = TLf[fq * nb + a];
+                    const double g_ = gap[fq] * tf, r_ = rhp[fq] * tf;
+#pragma unroll
+                    for (int e = 0; e < nb; ++e)
+                      acc[e] += g_ * phi_f[fq * nb + e] + r_ * RTr[fq * nb + e];
+                  }
+#pragma unroll
+                for (int e = 0; e < nb; ++e)
+                  srow[cj * nb + e] = acc[e];
+              }
+          }
+        // Row equilibration: S' = D S with D = diag(1/max|row|).  The sweep
+        // below inverts S'; S^-1 = S'^-1 D, so column k of the inverse is
+        // scaled by the factor of row p_k before it multiplies R.
+        double rscale;
+        {
+          double mx = 0.;
+#pragma unroll
+          for (int j = 0; j < NSMAX; ++j)
+            mx = fmax(mx, fabs(srow[j]));
+          rscale = (mx > 0.) ? 1. / mx : 1.;
+#pragma unroll
+          for (int j = 0; j < NSMAX; ++j)
+            srow[j] *= rscale;
+        }
+        // Sweep (exchange) form of Gauss-Jordan with virtual partial
+        // pivoting: exchanging unknown j with equation p_j.  Afterwards lane
+        // p_j holds row j of S'^-1 with its column k belonging to equation
+        // p_k.
+        bool used  = !act;
+        int  mypos = 0;
+        bool sing  = false;
+#pragma unroll
+        for (int j = 0; j < NSMAX; ++j)
+          {
+            if (j < Ns)
+              {
+                double best = used ? -1. : fabs(srow[j]);
+                int    bl   = lane;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+                  {
+                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int    oi = __shfl_xor_sync(0xffffffffu, bl, o);
+                    if (ob > best || (ob == best && oi < bl))
+                      {
+                        best = ob;
+                        bl   = oi;
+                      }
+                  }
+                sing |= !(best > 0.) || !isfinite(best);
+                const double pj = __shfl_sync(0xffffffffu, srow[j], bl);
+                const double hr = (pj != 0.) ? 1. / pj : 0.;
+                const bool   me = lane == bl;
+                const double l  = srow[j] * hr;
+#pragma unroll
+                for (int k = 0; k < NSMAX; ++k)
+                  {
+                    if (k == j)
+                      continue;
+                    const double pk = __shfl_sync(0xffffffffu, srow[k], bl);
+                    srow[k]         = me ? -pk * hr : srow[k] - l * pk;
+                  }
+                srow[j] = me ? hr : l;
+                if (me)
+                  {
+                    used  = true;
+                    mypos = j;
+                  }
+                if (lane == 0)
+                  piv3[warp][j] = bl;
+              }
+          }
+        if (sing && lane == 0)
+          atomicExch(P.status, 3);
+        // fold the row scaling of equation p_k into column k
+        {
+          double dsc[NSMAX];
+#pragma unroll
+          for (int k = 0; k < NSMAX; ++k)
+            dsc[k] = __shfl_sync(0xffffffffu, rscale, k < Ns ? piv3[warp][k] : 0);
+#pragma unroll
+          for (int k = 0; k < NSMAX; ++k)
+            srow[k] *= dsc[k];
+        }
+        __syncwarp();
+
+        // ---------- Y = S^-1 R, row mypos per lane, written back over R
+        for (int c0_ = 0; c0_ < ncol; c0_ += 16)
+          {
+            double acc[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u)
+              acc[u] = 0.;
+            if (act)
+              {
+#pragma unroll
+                for (int k = 0; k < NSMAX; ++k)
+                  if (k < Ns)
+                    {
+                      const double  sk = srow[k];
+                      const double *rk = R + piv3[warp][k] * ncol + c0_;
+#pragma unroll
+                      for (int u = 0; u < 16; ++u)
+                        if (c0_ + u < ncol)
+                          acc[u] += sk * rk[u];
+                    }
+              }
+            __syncwarp();
+            if (act)
+              {
+#pragma unroll
+                for (int u = 0; u < 16; ++u)
+                  if (c0_ + u < ncol)
+                    R[mypos * ncol + c0_ + u] = acc[u];
+              }
+            __syncwarp();
+          }
+        double *const Y = R;
+
+        // ------------------------ keep Y for the reconstruction [col][row]
+        {
+          double *yc = P.ycache + cell * (int64_t)Ns * P.ycols;
+          for (int idx = lane; idx < Ns * P.ycols; idx += 32)
+            yc[idx] = Y[(idx % Ns) * ncol + idx / Ns];
+        }
+        // combined residual column with the Dirichlet columns folded in
+        for (int j = lane; j < Ns; j += 32)
+          {
+            double acc = Y[j * ncol];
+            for (int t = 0; t < Nt; ++t)
+              if (dfl[t] != 0.)
+                {
+                  double y = Y[j * ncol + 1 + t];
+                  if (two)
+                    y += Y[j * ncol + 1 + Nt + t];
+                  acc -= gv[t] * y;
+                }
+            Yc[j] = acc;
+          }
+        __syncwarp();
+
+        // -------- trace rows: T = tc_c + tc_W P in registers, tt = T Y + ...
+        double *tt_out = P.tt + cell * (int64_t)Nt * Nt;
+        for (int i = lane; i < Nt; i += 32)
+          {
+            const int  fi = i / (ncomp * nf), ci2 = (i / nf) % ncomp, mi = i % nf;
+            const int  b  = cmp[ci2];
+            const bool rowD = dfl[i] != 0.;
+            double     Tr[NSMAX];
+#pragma unroll
+            for (int j = 0; j < NSMAX; ++j)
+              {
+                double v = 0.;
+                if (j < Ns)
+                  {
+                    const int cj = j / nb, e = j % nb;
+                    const int pr = b * 3 + cmp[cj];
+#pragma unroll
+                    for (int qf = 0; qf < nqf; ++qf)
+                      {
+                        const int fq = fi * nqf + qf;
+                        double    z  = tcW[pr * Fq + fq] * RTr[fq * nb + e];
+                        if (cj == ci2)
+                          z += tcS[b * Fq + fq] * phi_f[fq * nb + e];
+                        v += w_f[fq] * xi[qf * nf + mi] * z;
+                      }
+                  }
+                Tr[j] = v;
+              }
+            // rhs
+            double r = 0.;
+            if (!rowD)
+              {
+#pragma unroll
+                for (int j = 0; j < NSMAX; ++j)
+                  if (j < Ns)
+                    r += Tr[j] * Yc[j];
+#pragma unroll
+                for (int qf = 0; qf < nqf; ++qf)
+                  {
+                    const int fq = fi * nqf + qf;
+                    double    z  = rhsf[b * Fq + fq];
+                    for (int cp = 0; cp < ncomp; ++cp)
+                      z += tcW[(b * 3 + cmp[cp]) * Fq + fq] * Wrf[cp * Fq + fq];
+                    for (int t = 0; t < Nt; ++t)
+                      if (dfl[t] != 0.)
+                        {
+                          const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
+                          z -= gv[t] * tcW[(b * 3 + cmp[ct]) * Fq + fq] * RQr[fq * Ft + ft * nf + mt];
+                        }
+                    r += w_f[fq] * xi[qf * nf + mi] * z;
+                  }
+              }
+            P.rhs[cell * Nt + i]   = r;
+            P.dflag[cell * Nt + i] = rowD ? 1 : 0;
+            P.dval[cell * Nt + i]  = gv[i];
+            // tt row i, four columns at a time
+            double *ttr = tt_out + (int64_t)i * Nt;
+            for (int t0 = 0; t0 < Nt; t0 += 4)
+              {
+                double x[4] = {0., 0., 0., 0.};
+                if (!rowD)
+                  {
+#pragma unroll
+                    for (int j = 0; j < NSMAX; ++j)
+                      if (j < Ns)
+                        {
+                          const double *yj = Y + j * ncol + 1 + t0;
+#pragma unroll
+                          for (int u = 0; u < 4; ++u)
+                            if (t0 + u < Nt)
+                              {
+                                double y = yj[u];
+                                if (two)
+                                  y += yj[Nt + u];
+                                x[u] += Tr[j] * y;
+                              }
+                        }
+                  }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                  {
+                    const int t = t0 + u;
+                    if (t >= Nt)
+                      break;
+                    double o = 0.;
+                    if (!rowD && dfl[t] == 0.)
+                      {
+                        const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
+                        const int tq = ft * nf + mt;
+                        const int pr = b * 3 + cmp[ct];
+                        double    z  = x[u];
+#pragma unroll
+                        for (int qf = 0; qf < nqf; ++qf)
+                          {
+                            const int fq = fi * nqf + qf;
+                            double    v  = tcW[pr * Fq + fq] * RQr[fq * Ft + tq];
+                            if (ft == fi && ct == ci2)
+                              v += ttc[b * Fq + fq] * xi[qf * nf + mt];
+                            z += w_f[fq] * xi[qf * nf + mi] * v;
+                          }
+                        o = z;
+                      }
+                    ttr[t] = o;
+                  }
+              }
+          }
+        __syncwarp();
+      }
+  }
+} // namespace ddhdg

@@ -49,6 +49,7 @@ namespace ddhdg
     const double *cell_state, *trace_state;
     // outputs
     double  *tt, *rhs, *dval, *ycache;
+    double  *rscratch; // per-CTA R blocks when they do not fit in shared memory, or null
     int32_t *dflag;
     int     *status;
   };
