@@ -26,7 +26,7 @@ EXPORTS = [
     "ddhdg_set_enabled", "ddhdg_assemble_condense", "ddhdg_scatter", "ddhdg_get_csr",
     "ddhdg_solve_trace", "ddhdg_reconstruct", "ddhdg_newton", "ddhdg_last_timings",
     "ddhdg_project_cell", "ddhdg_project_trace", "ddhdg_project_density",
-    "ddhdg_reference_points", "ddhdg_last_error",
+    "ddhdg_reference_points", "ddhdg_last_error", "ddhdg_assemble_condense_noalloc",
 ]
 
 
@@ -84,6 +84,7 @@ def load(build_if_missing: bool = True):
     L.ddhdg_set_enabled.argtypes = [c_void_p, c_int, c_int, c_int]
     L.ddhdg_assemble_condense.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
                                           c_void_p, c_void_p, c_void_p]
+    L.ddhdg_assemble_condense_noalloc.argtypes = L.ddhdg_assemble_condense.argtypes
     L.ddhdg_scatter.argtypes = [c_void_p] + [c_void_p] * 6 + [c_int, c_void_p]
     L.ddhdg_get_csr.argtypes = [c_void_p, c_int, P(c_void_p), P(c_void_p)]
     L.ddhdg_solve_trace.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]

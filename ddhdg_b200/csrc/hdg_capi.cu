@@ -15,6 +15,7 @@
 #include <cstring>
 #include <functional>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -1383,6 +1384,138 @@ ddhdg_project_density(ddhdg_ctx *c, int comp, double qf, double *cell_state,
   project_trace_kernel<<<grid_for(c, c->nfaces, 128), 128, 0, (cudaStream_t)stream>>>(
     c->nfaces, c->dim, c->nb, c->nf, c->nqf, c->F, c->tables.p, c->to, nullptr, comp,
     trace_state, 1, cell_state, c->d_face_cells.p, c->d_face_local.p);
+  CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// ddhdg_assemble_condense_noalloc: the condense launch of
+// ddhdg_assemble_condense with its scratch (the per-cell Y cache and, for
+// cells whose right-hand-side block does not fit in shared memory, that
+// block) in a fixed static device array instead of context-owned buffers,
+// so that the call allocates no device memory.
+
+static __device__ __align__(256) double
+  ddhdg_noalloc_scratch[DDHDG_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+namespace
+{
+  constexpr int NoAllocMaxDevices = 64;
+  std::mutex    noalloc_mutex;
+  double       *noalloc_ptr[NoAllocMaxDevices] = {};
+
+  // Device address of the static scratch on the current device, looked up
+  // once per device (the first call on a device must come before any stream
+  // capture begins).
+  int
+  noalloc_scratch(double **out)
+  {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NoAllocMaxDevices)
+      return fail(DDHDG_BAD_ARG, "device ordinal beyond the no-allocation scratch table");
+    std::lock_guard<std::mutex> lock(noalloc_mutex);
+    if (!noalloc_ptr[dev])
+      {
+        void             *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, ddhdg_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+          {
+            cudaGetLastError();
+            return fail(DDHDG_CUDA_ERROR, std::string("cudaGetSymbolAddress of the static scratch: ") +
+                                            cudaGetErrorString(e));
+          }
+        noalloc_ptr[dev] = static_cast<double *>(p);
+      }
+    *out = noalloc_ptr[dev];
+    return DDHDG_OK;
+  }
+} // namespace
+
+extern "C" {
+
+int
+ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
+                                const double *trace_state, int thermo, double *tt,
+                                double *rhs, int32_t *dflag, double *dval,
+                                ddhdg_stream_t stream)
+{
+  if (!c || !cell_state || !trace_state || !tt || !rhs || !dflag || !dval)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo  = thermo ? 1 : 0;
+  Mode &m = c->mode[thermo];
+  if (!m.built)
+    set_mode_comps(c, thermo); // host bookkeeping only; no trace sparsity needed here
+  CondenseFn    cf;
+  ReconstructFn rf;
+  if (!kernels_for(c->dim, c->k, cf, rf))
+    return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
+  int     r;
+  KParams P     = make_params(c, thermo);
+  P.cell_state  = cell_state;
+  P.trace_state = trace_state;
+  P.tt          = tt;
+  P.rhs         = rhs;
+  P.dflag       = dflag;
+  P.dval        = dval;
+  const int64_t Ns = (int64_t)m.ncomp * c->nb;
+  int           threads;
+  size_t        smem;
+  int64_t       units;
+  bool          r_global = false;
+  if (3 * c->nb <= 32)
+    {
+      const Ws3Off w   = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol);
+      const size_t per = (size_t)w.total * sizeof(double);
+      int          wpb = (int)std::min<size_t>(Condense3MaxWPB, (220 * 1024) / per);
+      if (wpb < 1)
+        return fail(DDHDG_BAD_ARG, "the per-cell workspace does not fit in shared memory");
+      P.wpb   = wpb;
+      P.stage = 0;
+      threads = wpb * 32;
+      smem    = (size_t)wpb * per;
+      units   = (c->ncells + wpb - 1) / wpb;
+    }
+  else
+    {
+      int chunk, stage;
+      if ((r = launch_shape(c, m, chunk, stage, r_global, smem)))
+        return r;
+      P.wpb   = 1;
+      P.chunk = chunk;
+      P.stage = stage;
+      threads = CondenseTPB;
+      units   = c->ncells;
+    }
+  CK(cudaFuncSetAttribute(cf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, threads, smem));
+  if (per_sm < 1)
+    return fail(DDHDG_BAD_ARG, "condense kernel does not fit on an SM");
+  const int grid = (int)std::min<int64_t>(units, (int64_t)per_sm * c->sm_count);
+
+  // scratch: Y cache [ncells][Ns][ycols], then (256-byte aligned) one R block
+  // [Ns][ncol] per CTA when R lives outside shared memory
+  const size_t ycache_n = (size_t)c->ncells * Ns * m.ycols;
+  const size_t r_off    = (ycache_n + 31) & ~(size_t)31;
+  const size_t need_n   = r_global ? r_off + (size_t)grid * Ns * m.ncol : ycache_n;
+  if (need_n * sizeof(double) > DDHDG_NOALLOC_SCRATCH_BYTES)
+    return fail(DDHDG_BAD_ARG,
+                "this problem needs " + std::to_string(need_n * sizeof(double)) +
+                  " bytes of condensation scratch; ddhdg_assemble_condense_noalloc holds at most " +
+                  std::to_string((size_t)DDHDG_NOALLOC_SCRATCH_BYTES) +
+                  " bytes (use ddhdg_assemble_condense)");
+  double *scratch = nullptr;
+  if ((r = noalloc_scratch(&scratch)))
+    return r;
+  P.ycache   = scratch;
+  P.rscratch = r_global ? scratch + r_off : nullptr;
+
+  // the status word must start at zero (a singular local system sets it)
+  CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), (cudaStream_t)stream));
+  cf<<<grid, threads, smem, (cudaStream_t)stream>>>(P);
   CK(cudaGetLastError());
   return DDHDG_OK;
 }

@@ -149,6 +149,33 @@ int ddhdg_assemble_condense(ddhdg_ctx *ctx, const double *cell_state,
                             double *tt, double *rhs, int32_t *dflag,
                             double *dval, ddhdg_stream_t stream);
 
+/* Fixed size of the static scratch of ddhdg_assemble_condense_noalloc. */
+#define DDHDG_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* No counterpart in the reference.  The same per-cell outputs as
+ * ddhdg_assemble_condense, from a call that allocates no device memory: the
+ * kernel's scratch (the per-cell Y cache and, for cells whose right-hand-side
+ * block does not fit in shared memory, that block) lives in a static device
+ * array of DDHDG_NOALLOC_SCRATCH_BYTES (16 MiB) inside the library.
+ * It is for callers that cannot allocate device memory at this point: a
+ * process whose device memory is already held by its own pool allocator (a
+ * framework's caching allocator), where a cudaMalloc inside the library would
+ * fail or fragment that pool, and latency-bound loops that cannot take the
+ * device-wide synchronisation of cudaFree.
+ * Limits.  A problem that needs more scratch than 16 MiB (about 2000 cells of
+ * the 2D degree-2 three-component system) is rejected with DDHDG_BAD_ARG
+ * before anything is launched.  The first call on each device looks up the
+ * array's address (cudaGetSymbolAddress, with that device current); that
+ * first call must happen before any stream capture begins.  All calls on one
+ * device share the one array and the context's status word: overlapping calls
+ * (several threads, or several streams in flight) race.  The Y cache written
+ * here is not the one ddhdg_reconstruct reads; reconstruction still follows
+ * ddhdg_assemble_condense. */
+int ddhdg_assemble_condense_noalloc(ddhdg_ctx *ctx, const double *cell_state,
+                                    const double *trace_state, int thermo_eq,
+                                    double *tt, double *rhs, int32_t *dflag,
+                                    double *dval, ddhdg_stream_t stream);
+
 /* copy_local_to_global (src/np_solver.cpp:1293-1322): scatter the per-cell
  * condensed systems into the global CSR trace matrix (values[nnz], rows and
  * columns from ddhdg_get_csr) and rhs[n_trace_dofs]; Dirichlet rows become
