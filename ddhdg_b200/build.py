@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libddhdg_b200.so")
 SOURCES = ["hdg_capi.cu"]
-DEPS = SOURCES + ["hdg_kernels.cuh", "hdg_tables.h", os.path.join("..", "..", "include", "ddhdg_b200.h")]
+HEADER = os.path.join(HERE, "..", "include", "ddhdg_b200.h")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -26,7 +26,8 @@ def needs_build():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    return any(os.path.getmtime(os.path.join(CSRC, d)) > t for d in DEPS)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))]
+    return any(os.path.getmtime(d) > t for d in deps + [HEADER])
 
 
 def build(force=False, verbose=False):

@@ -5,12 +5,14 @@
 // Same mathematics as condense2_kernel (hdg_condense.cuh): the flux unknowns
 // are eliminated through the constant mass matrix and the scalar system
 // S y = R of the enabled components is solved for the residual and for every
-// trace dof.  The difference is the execution model: every lane owns one row
-// of the local system in registers, the Gauss-Jordan inverse of S runs with
-// warp shuffles (virtual partial pivoting, no barriers), and the products
-// Y = S^-1 R and tt = T Y are formed with per-lane register accumulators, so
-// that each lane has tens of independent FMAs in flight.  Warps are
-// independent; the constant tables are read through the L1 cache.
+// trace dof.  The execution model differs: every lane owns one row of S in
+// registers and the Gauss-Jordan inverse runs as a short loop of warp
+// shuffles (virtual partial pivoting; the register row is rotated by one
+// position per step so that the current column is always register 0);
+// Y = S^-1 R is formed with per-lane register accumulators; and the condensed
+// trace matrix tt = T Y + (face terms) is a register-tiled product on a 4 x 8
+// lane grid.  Warps are independent; the constant tables are read through
+// the L1 cache.
 #pragma once
 
 #include <cstdint>
@@ -24,15 +26,20 @@ namespace ddhdg
 
   struct Ws3Off
   {
-    int coef, lam, c0, W0, qc, c0f, W0n, tr0, Wrc, Wrf, tau, bcs;
-    int al, be, ka, ga, rh, ctc, ctd, tcS, tcW, ttc, rhsf, r0, r1, rf;
-    int R, g, dfl, Yc, total;
+    // dead once Y is formed; the trace-row arrays below overlay them
+    int coef, lam, c0, W0, qc, c0f, W0n, tr0, Wrc, tau, bcs;
+    int al, be, ka, ga, rh, ctc, ctd, r0, r1, rf;
+    // trace-row data of the condensation (overlay)
+    int Trs, rA, rS, rD, rZ, H;
+    // live to the end of the cell
+    int tcS, tcW, ttc, rhsf, Wrf, R, g, dfl, Yc, total;
+    int ldr; // row stride of R / Y (even: 16-byte aligned rows)
   };
 
   __host__ __device__ inline Ws3Off
   ws3_layout(int dim, int nb, int nf, int ncomp, int ncol)
   {
-    const int F = 2 * dim, nqc = nb, Fq = F * nf;
+    const int F = 2 * dim, nqc = nb, Fq = F * nf, nqf = nf;
     const int Ns = ncomp * nb, Nt = F * ncomp * nf;
     Ws3Off    o;
     int       p = 0;
@@ -41,36 +48,46 @@ namespace ddhdg
       p += (n + 1) & ~1;
       return r;
     };
-    o.coef  = take(3 * (dim + 1) * nb);
-    o.lam   = take(F * 3 * nf);
-    o.c0    = take(3 * nqc);
-    o.W0    = take(3 * dim * nqc);
-    o.qc    = take(6 * nqc);
-    o.c0f   = take(3 * Fq);
-    o.W0n   = take(3 * Fq);
-    o.tr0   = take(3 * Fq);
-    o.Wrc   = take(3 * dim * nqc);
-    o.Wrf   = take(3 * Fq);
-    o.tau   = take(F * 3);
-    o.bcs   = take(F * 3);
-    o.al    = take(9 * nqc);
-    o.be    = take(9 * nqc * dim);
-    o.ka    = take(9 * nqc);
-    o.ga    = take(9 * Fq);
-    o.rh    = take(9 * Fq);
-    o.ctc   = take(3 * Fq);
-    o.ctd   = take(3 * Fq);
-    o.tcS   = take(3 * Fq);
-    o.tcW   = take(9 * Fq);
-    o.ttc   = take(3 * Fq);
-    o.rhsf  = take(3 * Fq);
-    o.r0    = take(3 * nqc);
-    o.r1    = take(3 * nqc * dim);
-    o.rf    = take(3 * Fq);
-    o.R     = take(Ns * ncol);
-    o.g     = take(Nt);
-    o.dfl   = take(Nt);
-    o.Yc    = take(Ns);
+    o.coef = take(3 * (dim + 1) * nb);
+    o.lam  = take(F * 3 * nf);
+    o.c0   = take(3 * nqc);
+    o.W0   = take(3 * dim * nqc);
+    o.qc   = take(6 * nqc);
+    o.c0f  = take(3 * Fq);
+    o.W0n  = take(3 * Fq);
+    o.tr0  = take(3 * Fq);
+    o.Wrc  = take(3 * dim * nqc);
+    o.tau  = take(F * 3);
+    o.bcs  = take(F * 3);
+    o.al   = take(9 * nqc);
+    o.be   = take(9 * nqc * dim);
+    o.ka   = take(9 * nqc);
+    o.ga   = take(9 * Fq);
+    o.rh   = take(9 * Fq);
+    o.ctc  = take(3 * Fq);
+    o.ctd  = take(3 * Fq);
+    o.r0   = take(3 * nqc);
+    o.r1   = take(3 * nqc * dim);
+    o.rf   = take(3 * Fq);
+    const int dead_end = p;
+    p     = 0;
+    o.Trs = take(Ns * Nt);
+    o.rA  = take(Nt * 3 * nqf);
+    o.rS  = take(Nt * nqf);
+    o.rD  = take(Nt * nqf);
+    o.rZ  = take(Nt);
+    o.H   = take(3 * Fq);
+    p     = p > dead_end ? p : dead_end;
+    o.tcS  = take(3 * Fq);
+    o.tcW  = take(9 * Fq);
+    o.ttc  = take(3 * Fq);
+    o.rhsf = take(3 * Fq);
+    o.Wrf  = take(3 * Fq);
+    o.ldr  = (ncol + 1) & ~1;
+    o.R    = take(Ns * o.ldr);
+    o.g    = take(Nt);
+    o.dfl  = take(Nt);
+    o.Yc   = take(Ns);
     o.total = p;
     return o;
   }
@@ -90,7 +107,7 @@ namespace ddhdg
     constexpr int NCA   = Dm::Nc_all;
     constexpr int NSMAX = 3 * nb;
     static_assert(NSMAX <= 32, "one lane per row of the scalar system");
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     __shared__ int piv3[Condense3MaxWPB][NSMAX];
 
     const int  lane  = threadIdx.x & 31;
@@ -129,6 +146,10 @@ namespace ddhdg
            *tcW = ws + wo.tcW, *ttc = ws + wo.ttc, *rhsf = ws + wo.rhsf, *r0 = ws + wo.r0,
            *r1 = ws + wo.r1, *rf = ws + wo.rf, *R = ws + wo.R,
            *gv = ws + wo.g, *dfl = ws + wo.dfl, *Yc = ws + wo.Yc;
+    double *Trs = ws + wo.Trs, *rA = ws + wo.rA, *rS = ws + wo.rS, *rD = ws + wo.rD,
+           *rZ = ws + wo.rZ, *Hs = ws + wo.H;
+    const int ldr  = wo.ldr;
+    const int colC = two ? 1 + Nt : 1; // combined trace columns of Y
 
     const double eps = P.eps, mun = P.mun, mup = P.mup, U_T = P.U_T;
     const bool   thermo   = P.thermo != 0;
@@ -549,7 +570,7 @@ namespace ddhdg
 #pragma unroll
               for (int fq = 0; fq < Fq; ++fq)
                 v += TLf[fq * nb + a] * rfp[fq];
-              R[lane * ncol] = v;
+              R[lane * ldr] = v;
             }
             // trace columns, one trial component at a time
             for (int cj = 0; cj < ncomp; ++cj)
@@ -600,15 +621,17 @@ namespace ddhdg
                 for (int f = 0; f < F; ++f)
 #pragma unroll
                   for (int m = 0; m < nf; ++m)
-                    R[lane * ncol + 1 + (f * ncomp + cj) * nf + m] = acc[f * nf + m];
+                    R[lane * ldr + 1 + (f * ncomp + cj) * nf + m] = acc[f * nf + m];
                 if (two)
                   {
+                    // drift columns are only used added to the trace columns:
+                    // keep them combined (ct_cell + ct_drift)
 #pragma unroll
                     for (int f = 0; f < F; ++f)
 #pragma unroll
                       for (int m = 0; m < nf; ++m)
                         {
-                          double d = 0.;
+                          double d = acc[f * nf + m];
                           if (cj == ci)
 #pragma unroll
                             for (int qf = 0; qf < nqf; ++qf)
@@ -616,17 +639,19 @@ namespace ddhdg
                                 const int fq = f * nqf + qf;
                                 d += ctd[bi * Fq + fq] * TLf[fq * nb + a] * xi[qf * nf + m];
                               }
-                          R[lane * ncol + 1 + Nt + (f * ncomp + cj) * nf + m] = d;
+                          R[lane * ldr + 1 + Nt + (f * ncomp + cj) * nf + m] = d;
                         }
                   }
               }
           }
 
         // ------------ S row per lane, in-place Gauss-Jordan inverse
+        // lanes Ns..NSMAX-1 carry unit rows, so that the elimination always
+        // runs over NSMAX columns (S padded to diag(S, I))
         double srow[NSMAX];
 #pragma unroll
         for (int j = 0; j < NSMAX; ++j)
-          srow[j] = 0.;
+          srow[j] = (lane >= Ns && lane == j) ? 1. : 0.;
         if (act)
           {
 #pragma unroll
@@ -695,66 +720,63 @@ namespace ddhdg
             srow[j] *= rscale;
         }
         // Sweep (exchange) form of Gauss-Jordan with virtual partial
-        // pivoting: exchanging unknown j with equation p_j.  Afterwards lane
-        // p_j holds row j of S'^-1 with its column k belonging to equation
-        // p_k.
-        bool used  = !act;
+        // pivoting: step j exchanges unknown j with equation p_j.  The row is
+        // rotated left by one register per step, so column j sits in srow[0]
+        // at step j and NSMAX steps bring every column back to its place.
+        // Afterwards lane p_j holds row j of S'^-1, whose column k belongs to
+        // equation p_k.
+        bool used  = lane >= NSMAX;
         int  mypos = 0;
         bool sing  = false;
-#pragma unroll
+#pragma unroll 1
         for (int j = 0; j < NSMAX; ++j)
           {
-            if (j < Ns)
+            double best = used ? -1. : fabs(srow[0]);
+            int    bl   = lane;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
               {
-                double best = used ? -1. : fabs(srow[j]);
-                int    bl   = lane;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1)
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int    oi = __shfl_xor_sync(0xffffffffu, bl, o);
+                if (ob > best || (ob == best && oi < bl))
                   {
-                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                    const int    oi = __shfl_xor_sync(0xffffffffu, bl, o);
-                    if (ob > best || (ob == best && oi < bl))
-                      {
-                        best = ob;
-                        bl   = oi;
-                      }
+                    best = ob;
+                    bl   = oi;
                   }
-                sing |= !(best > 0.) || !isfinite(best);
-                const double pj = __shfl_sync(0xffffffffu, srow[j], bl);
-                const double hr = (pj != 0.) ? 1. / pj : 0.;
-                const bool   me = lane == bl;
-                const double l  = srow[j] * hr;
-#pragma unroll
-                for (int k = 0; k < NSMAX; ++k)
-                  {
-                    if (k == j)
-                      continue;
-                    const double pk = __shfl_sync(0xffffffffu, srow[k], bl);
-                    srow[k]         = me ? -pk * hr : srow[k] - l * pk;
-                  }
-                srow[j] = me ? hr : l;
-                if (me)
-                  {
-                    used  = true;
-                    mypos = j;
-                  }
-                if (lane == 0)
-                  piv3[warp][j] = bl;
               }
+            sing |= !(best > 0.) || !isfinite(best);
+            const double pj = __shfl_sync(0xffffffffu, srow[0], bl);
+            const double hr = (pj != 0.) ? 1. / pj : 0.;
+            const bool   me = lane == bl;
+            const double l  = srow[0] * hr;
+#pragma unroll
+            for (int k = 1; k < NSMAX; ++k)
+              {
+                const double pk = __shfl_sync(0xffffffffu, srow[k], bl);
+                srow[k - 1]     = me ? -pk * hr : srow[k] - l * pk;
+              }
+            srow[NSMAX - 1] = me ? hr : l;
+            if (me)
+              {
+                used  = true;
+                mypos = j;
+              }
+            if (lane == 0)
+              piv3[warp][j] = bl;
           }
         if (sing && lane == 0)
           atomicExch(P.status, 3);
+        __syncwarp();
         // fold the row scaling of equation p_k into column k
         {
           double dsc[NSMAX];
 #pragma unroll
           for (int k = 0; k < NSMAX; ++k)
-            dsc[k] = __shfl_sync(0xffffffffu, rscale, k < Ns ? piv3[warp][k] : 0);
+            dsc[k] = __shfl_sync(0xffffffffu, rscale, piv3[warp][k]);
 #pragma unroll
           for (int k = 0; k < NSMAX; ++k)
             srow[k] *= dsc[k];
         }
-        __syncwarp();
 
         // ---------- Y = S^-1 R, row mypos per lane, written back over R
         for (int c0_ = 0; c0_ < ncol; c0_ += 16)
@@ -769,12 +791,17 @@ namespace ddhdg
                 for (int k = 0; k < NSMAX; ++k)
                   if (k < Ns)
                     {
-                      const double  sk = srow[k];
-                      const double *rk = R + piv3[warp][k] * ncol + c0_;
+                      const double   sk = srow[k];
+                      const double2 *rk =
+                        reinterpret_cast<const double2 *>(R + piv3[warp][k] * ldr + c0_);
 #pragma unroll
-                      for (int u = 0; u < 16; ++u)
-                        if (c0_ + u < ncol)
-                          acc[u] += sk * rk[u];
+                      for (int v = 0; v < 8; ++v)
+                        if (c0_ + 2 * v < ncol)
+                          {
+                            const double2 x = rk[v];
+                            acc[2 * v] += sk * x.x;
+                            acc[2 * v + 1] += sk * x.y;
+                          }
                     }
               }
             __syncwarp();
@@ -783,7 +810,7 @@ namespace ddhdg
 #pragma unroll
                 for (int u = 0; u < 16; ++u)
                   if (c0_ + u < ncol)
-                    R[mypos * ncol + c0_ + u] = acc[u];
+                    R[mypos * ldr + c0_ + u] = acc[u];
               }
             __syncwarp();
           }
@@ -791,132 +818,197 @@ namespace ddhdg
 
         // ------------------------ keep Y for the reconstruction [col][row]
         {
-          double *yc = P.ycache + cell * (int64_t)Ns * P.ycols;
-          for (int idx = lane; idx < Ns * P.ycols; idx += 32)
-            yc[idx] = Y[(idx % Ns) * ncol + idx / Ns];
+          double   *yc  = P.ycache + cell * (int64_t)Ns * P.ycols;
+          const int tot = Ns * P.ycols;
+          int       row = lane % Ns, col = lane / Ns;
+          for (int idx = lane; idx < tot; idx += 32)
+            {
+              yc[idx] = Y[row * ldr + col];
+              row += 32;
+              while (row >= Ns)
+                {
+                  row -= Ns;
+                  ++col;
+                }
+            }
         }
         // combined residual column with the Dirichlet columns folded in
         for (int j = lane; j < Ns; j += 32)
           {
-            double acc = Y[j * ncol];
+            double acc = Y[j * ldr];
             for (int t = 0; t < Nt; ++t)
               if (dfl[t] != 0.)
-                {
-                  double y = Y[j * ncol + 1 + t];
-                  if (two)
-                    y += Y[j * ncol + 1 + Nt + t];
-                  acc -= gv[t] * y;
-                }
+                acc -= gv[t] * Y[j * ldr + colC + t];
             Yc[j] = acc;
+          }
+        __syncwarp(); // the coefficient arrays are dead from here on
+
+        // ------------- trace-row data: face weights, H = Wrf - Dirichlet flux
+        for (int idx = lane; idx < ncomp * Fq; idx += 32)
+          {
+            const int cp = idx / Fq, fq = idx % Fq;
+            double    h  = Wrf[idx];
+#pragma unroll
+            for (int ft = 0; ft < F; ++ft)
+#pragma unroll
+              for (int mt = 0; mt < nf; ++mt)
+                {
+                  const int t = (ft * ncomp + cp) * nf + mt;
+                  if (dfl[t] != 0.)
+                    h -= gv[t] * RQr[fq * Ft + ft * nf + mt];
+                }
+            Hs[idx] = h;
+          }
+        __syncwarp();
+        for (int i = lane; i < Nt; i += 32)
+          {
+            const int fi = i / (ncomp * nf), ci2 = (i / nf) % ncomp, mi = i % nf;
+            const int b  = cmp[ci2];
+            double    z  = 0.;
+#pragma unroll
+            for (int qf = 0; qf < nqf; ++qf)
+              {
+                const int    fq = fi * nqf + qf;
+                const double w  = w_f[fq] * xi[qf * nf + mi];
+                rS[i * nqf + qf] = w * tcS[b * Fq + fq];
+                rD[i * nqf + qf] = w * ttc[b * Fq + fq];
+                z += w * rhsf[b * Fq + fq];
+                for (int cp = 0; cp < ncomp; ++cp)
+                  {
+                    const double tw = w * tcW[(b * 3 + cmp[cp]) * Fq + fq];
+                    rA[(i * 3 + cp) * nqf + qf] = tw;
+                    z += tw * Hs[cp * Fq + fq];
+                  }
+              }
+            rZ[i] = z;
           }
         __syncwarp();
 
-        // -------- trace rows: T = tc_c + tc_W P in registers, tt = T Y + ...
-        double *tt_out = P.tt + cell * (int64_t)Nt * Nt;
-        for (int i = lane; i < Nt; i += 32)
+        // --------- reduced trace operator T = tc_c + tc_W P, stored [j][i]
+        for (int idx = lane; idx < Nt * ncomp; idx += 32)
           {
-            const int  fi = i / (ncomp * nf), ci2 = (i / nf) % ncomp, mi = i % nf;
-            const int  b  = cmp[ci2];
-            const bool rowD = dfl[i] != 0.;
-            double     Tr[NSMAX];
+            const int i = idx / ncomp, cj = idx - i * ncomp;
+            const int fi = i / (ncomp * nf), ci2 = (i / nf) % ncomp;
+            double    wa[nqf], ws_[nqf];
 #pragma unroll
-            for (int j = 0; j < NSMAX; ++j)
+            for (int qf = 0; qf < nqf; ++qf)
+              {
+                wa[qf]  = rA[(i * 3 + cj) * nqf + qf];
+                ws_[qf] = (cj == ci2) ? rS[i * nqf + qf] : 0.;
+              }
+#pragma unroll
+            for (int e = 0; e < nb; ++e)
               {
                 double v = 0.;
-                if (j < Ns)
-                  {
-                    const int cj = j / nb, e = j % nb;
-                    const int pr = b * 3 + cmp[cj];
-#pragma unroll
-                    for (int qf = 0; qf < nqf; ++qf)
-                      {
-                        const int fq = fi * nqf + qf;
-                        double    z  = tcW[pr * Fq + fq] * RTr[fq * nb + e];
-                        if (cj == ci2)
-                          z += tcS[b * Fq + fq] * phi_f[fq * nb + e];
-                        v += w_f[fq] * xi[qf * nf + mi] * z;
-                      }
-                  }
-                Tr[j] = v;
-              }
-            // rhs
-            double r = 0.;
-            if (!rowD)
-              {
-#pragma unroll
-                for (int j = 0; j < NSMAX; ++j)
-                  if (j < Ns)
-                    r += Tr[j] * Yc[j];
 #pragma unroll
                 for (int qf = 0; qf < nqf; ++qf)
                   {
                     const int fq = fi * nqf + qf;
-                    double    z  = rhsf[b * Fq + fq];
-                    for (int cp = 0; cp < ncomp; ++cp)
-                      z += tcW[(b * 3 + cmp[cp]) * Fq + fq] * Wrf[cp * Fq + fq];
-                    for (int t = 0; t < Nt; ++t)
-                      if (dfl[t] != 0.)
-                        {
-                          const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
-                          z -= gv[t] * tcW[(b * 3 + cmp[ct]) * Fq + fq] * RQr[fq * Ft + ft * nf + mt];
-                        }
-                    r += w_f[fq] * xi[qf * nf + mi] * z;
+                    v += wa[qf] * RTr[fq * nb + e] + ws_[qf] * phi_f[fq * nb + e];
                   }
+                Trs[(cj * nb + e) * Nt + i] = v;
+              }
+          }
+        __syncwarp();
+
+        // ------------------------------------- right-hand side and flags
+        for (int i = lane; i < Nt; i += 32)
+          {
+            const bool rowD = dfl[i] != 0.;
+            double     r    = 0.;
+            if (!rowD)
+              {
+                for (int j = 0; j < Ns; ++j)
+                  r += Trs[j * Nt + i] * Yc[j];
+                r += rZ[i];
               }
             P.rhs[cell * Nt + i]   = r;
             P.dflag[cell * Nt + i] = rowD ? 1 : 0;
             P.dval[cell * Nt + i]  = gv[i];
-            // tt row i, four columns at a time
-            double *ttr = tt_out + (int64_t)i * Nt;
-            for (int t0 = 0; t0 < Nt; t0 += 4)
-              {
-                double x[4] = {0., 0., 0., 0.};
-                if (!rowD)
-                  {
-#pragma unroll
-                    for (int j = 0; j < NSMAX; ++j)
-                      if (j < Ns)
-                        {
-                          const double *yj = Y + j * ncol + 1 + t0;
-#pragma unroll
-                          for (int u = 0; u < 4; ++u)
-                            if (t0 + u < Nt)
-                              {
-                                double y = yj[u];
-                                if (two)
-                                  y += yj[Nt + u];
-                                x[u] += Tr[j] * y;
-                              }
-                        }
-                  }
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-                  {
-                    const int t = t0 + u;
-                    if (t >= Nt)
-                      break;
-                    double o = 0.;
-                    if (!rowD && dfl[t] == 0.)
-                      {
-                        const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
-                        const int tq = ft * nf + mt;
-                        const int pr = b * 3 + cmp[ct];
-                        double    z  = x[u];
-#pragma unroll
-                        for (int qf = 0; qf < nqf; ++qf)
-                          {
-                            const int fq = fi * nqf + qf;
-                            double    v  = tcW[pr * Fq + fq] * RQr[fq * Ft + tq];
-                            if (ft == fi && ct == ci2)
-                              v += ttc[b * Fq + fq] * xi[qf * nf + mt];
-                            z += w_f[fq] * xi[qf * nf + mi] * v;
-                          }
-                        o = z;
-                      }
-                    ttr[t] = o;
-                  }
-              }
           }
+
+        // ------ tt = T Y_t + tc_W Q_t + face block, 4 x 8 lane grid of tiles
+        {
+          constexpr int NTM = F * 3 * nf;
+          constexpr int TC  = (NTM + 7) / 8;
+          constexpr int TR0 = (NTM + 3) / 4;
+          constexpr int TR  = TR0 < 9 ? TR0 : 9;
+          const int     lr = lane >> 3, lc = lane & 7;
+          double       *tt_out = P.tt + cell * (int64_t)Nt * Nt;
+          int           ft_[TC], ct_[TC], mt_[TC];
+          bool          cok[TC];
+#pragma unroll
+          for (int b = 0; b < TC; ++b)
+            {
+              const int t = lc + 8 * b;
+              ft_[b]      = t / (ncomp * nf);
+              ct_[b]      = (t / nf) % ncomp;
+              mt_[b]      = t % nf;
+              cok[b]      = t < Nt && dfl[t < Nt ? t : 0] == 0.;
+            }
+          for (int r0_ = 0; r0_ < Nt; r0_ += 4 * TR)
+            {
+              double acc[TR][TC];
+#pragma unroll
+              for (int a2 = 0; a2 < TR; ++a2)
+#pragma unroll
+                for (int b = 0; b < TC; ++b)
+                  acc[a2][b] = 0.;
+#pragma unroll 1
+              for (int j = 0; j < Ns; ++j)
+                {
+                  double ta[TR], yb[TC];
+#pragma unroll
+                  for (int a2 = 0; a2 < TR; ++a2)
+                    {
+                      const int i = r0_ + lr + 4 * a2;
+                      ta[a2]      = (i < Nt) ? Trs[j * Nt + i] : 0.;
+                    }
+#pragma unroll
+                  for (int b = 0; b < TC; ++b)
+                    {
+                      const int t = lc + 8 * b;
+                      yb[b]       = (t < Nt) ? Y[j * ldr + colC + t] : 0.;
+                    }
+#pragma unroll
+                  for (int a2 = 0; a2 < TR; ++a2)
+#pragma unroll
+                    for (int b = 0; b < TC; ++b)
+                      acc[a2][b] += ta[a2] * yb[b];
+                }
+#pragma unroll
+              for (int a2 = 0; a2 < TR; ++a2)
+                {
+                  const int i = r0_ + lr + 4 * a2;
+                  if (i >= Nt)
+                    continue;
+                  const int  fi = i / (ncomp * nf), ci2 = (i / nf) % ncomp;
+                  const bool rok = dfl[i] == 0.;
+#pragma unroll
+                  for (int b = 0; b < TC; ++b)
+                    {
+                      const int t = lc + 8 * b;
+                      if (t >= Nt)
+                        continue;
+                      double o = 0.;
+                      if (rok && cok[b])
+                        {
+                          const int tq = ft_[b] * nf + mt_[b];
+                          double    z  = acc[a2][b];
+#pragma unroll
+                          for (int qf = 0; qf < nqf; ++qf)
+                            z += rA[(i * 3 + ct_[b]) * nqf + qf] * RQr[(fi * nqf + qf) * Ft + tq];
+                          if (ft_[b] == fi && ct_[b] == ci2)
+#pragma unroll
+                            for (int qf = 0; qf < nqf; ++qf)
+                              z += rD[i * nqf + qf] * xi[qf * nf + mt_[b]];
+                          o = z;
+                        }
+                      tt_out[(int64_t)i * Nt + t] = o;
+                    }
+                }
+            }
+        }
         __syncwarp();
       }
   }
