@@ -454,24 +454,63 @@ namespace
     return P;
   }
 
-  using CondenseFn    = void (*)(KParams);
   using ReconstructFn = void (*)(KParams, const double *, double *);
+
+  // one condense kernel of a (dim, degree): its address (attributes,
+  // occupancy) and a launcher that builds its parameters
+  struct CondenseKernel
+  {
+    const void *fn = nullptr;
+    void (*launch)(const Tables &, const KParams &, int, int, size_t, cudaStream_t) = nullptr;
+  };
 
   template <int D, int K>
   void
-  pick(CondenseFn &cf, ReconstructFn &rf)
+  fill_ctab(const Tables &T, CTab<D, K> &C)
+  {
+    auto put = [](double *dst, size_t n, const std::vector<double> &src) {
+      std::memcpy(dst, src.data(), std::min(n, src.size()) * sizeof(double));
+    };
+    put(C.phi_c, sizeof(C.phi_c) / sizeof(double), T.phi_c);
+    put(C.RTk, sizeof(C.RTk) / sizeof(double), T.RTk);
+    put(C.phi_f, sizeof(C.phi_f) / sizeof(double), T.phi_f);
+    put(C.RTr, sizeof(C.RTr) / sizeof(double), T.RTr);
+    put(C.RQk, sizeof(C.RQk) / sizeof(double), T.RQk);
+    put(C.RQr, sizeof(C.RQr) / sizeof(double), T.RQr);
+    put(C.xi, sizeof(C.xi) / sizeof(double), T.xi);
+  }
+
+  template <int D, int K>
+  void
+  launch_condense(const Tables &T, const KParams &P, int grid, int threads, size_t smem,
+                  cudaStream_t s)
+  {
+    if constexpr (3 * Dims<D, K>::nb <= 32)
+      {
+        CTab<D, K> C;
+        fill_ctab(T, C);
+        condense3_kernel<D, K><<<grid, threads, smem, s>>>(P, C);
+      }
+    else
+      condense2_kernel<D, K><<<grid, threads, smem, s>>>(P);
+  }
+
+  template <int D, int K>
+  void
+  pick(CondenseKernel &cf, ReconstructFn &rf)
   {
     // warp-per-cell register kernel when one lane can own one row of the
     // scalar system, CTA-per-cell shared-memory kernel otherwise
     if constexpr (3 * Dims<D, K>::nb <= 32)
-      cf = condense3_kernel<D, K>;
+      cf.fn = reinterpret_cast<const void *>(condense3_kernel<D, K>);
     else
-      cf = condense2_kernel<D, K>;
-    rf = reconstruct_kernel<D, K>;
+      cf.fn = reinterpret_cast<const void *>(condense2_kernel<D, K>);
+    cf.launch = launch_condense<D, K>;
+    rf        = reconstruct_kernel<D, K>;
   }
 
   bool
-  kernels_for(int dim, int k, CondenseFn &cf, ReconstructFn &rf)
+  kernels_for(int dim, int k, CondenseKernel &cf, ReconstructFn &rf)
   {
     switch (dim * 10 + k)
       {
@@ -1042,7 +1081,7 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
   if ((r = ensure_buffers(c, thermo)))
     return r;
   Mode      &m = c->mode[thermo];
-  CondenseFn cf;
+  CondenseKernel cf;
   ReconstructFn rf;
   if (!kernels_for(c->dim, c->k, cf, rf))
     return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
@@ -1085,21 +1124,21 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
       if (r_global)
         {
           int per_sm = 0;
-          CK(cudaFuncSetAttribute(cf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-          CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, threads, smem));
+          CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, threads, smem));
           const int64_t g = std::min<int64_t>(units, (int64_t)std::max(per_sm, 1) * c->sm_count);
           if ((r = m.rscratch.alloc((size_t)g * c->nb * m.ncomp * m.ncol)))
             return r;
           P.rscratch = m.rscratch.p;
         }
     }
-  CK(cudaFuncSetAttribute(cf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, threads, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, threads, smem));
   if (per_sm < 1)
     return fail(DDHDG_BAD_ARG, "condense kernel does not fit on an SM");
   const int grid = (int)std::min<int64_t>(units, (int64_t)per_sm * c->sm_count);
-  cf<<<grid, threads, smem, (cudaStream_t)stream>>>(P);
+  cf.launch(c->T, P, grid, threads, smem, (cudaStream_t)stream);
   CK(cudaGetLastError());
   return DDHDG_OK;
 }
@@ -1115,7 +1154,7 @@ ddhdg_reconstruct(ddhdg_ctx *c, const double *cell_state, const double *trace_st
   Mode &m = c->mode[thermo];
   if (!m.built || !m.ycache.p)
     return fail(DDHDG_BAD_ARG, "ddhdg_reconstruct needs a preceding ddhdg_assemble_condense");
-  CondenseFn    cf;
+  CondenseKernel cf;
   ReconstructFn rf;
   if (!kernels_for(c->dim, c->k, cf, rf))
     return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
@@ -1448,7 +1487,7 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
   Mode &m = c->mode[thermo];
   if (!m.built)
     set_mode_comps(c, thermo); // host bookkeeping only; no trace sparsity needed here
-  CondenseFn    cf;
+  CondenseKernel cf;
   ReconstructFn rf;
   if (!kernels_for(c->dim, c->k, cf, rf))
     return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
@@ -1489,9 +1528,9 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
       threads = CondenseTPB;
       units   = c->ncells;
     }
-  CK(cudaFuncSetAttribute(cf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf, threads, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, threads, smem));
   if (per_sm < 1)
     return fail(DDHDG_BAD_ARG, "condense kernel does not fit on an SM");
   const int grid = (int)std::min<int64_t>(units, (int64_t)per_sm * c->sm_count);
@@ -1515,7 +1554,7 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
 
   // the status word must start at zero (a singular local system sets it)
   CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), (cudaStream_t)stream));
-  cf<<<grid, threads, smem, (cudaStream_t)stream>>>(P);
+  cf.launch(c->T, P, grid, threads, smem, (cudaStream_t)stream);
   CK(cudaGetLastError());
   return DDHDG_OK;
 }

@@ -24,6 +24,26 @@ namespace ddhdg
 {
   constexpr int Condense3MaxWPB = 8; // warps (cells) per CTA at most
 
+  // Constant tables read at lane-uniform addresses in fully unrolled loops.
+  // They travel as a kernel parameter (constant bank), so that the FMAs take
+  // them as constant operands; at most 14.4 KB (3D, degree 1).
+  template <int DIM, int K>
+  struct CTab
+  {
+    using Dm                 = Dims<DIM, K>;
+    static constexpr int nb  = Dm::nb;
+    static constexpr int nqc = Dm::nqc;
+    static constexpr int Fq  = Dm::F * Dm::nqf;
+    static constexpr int Ft  = Dm::F * Dm::nf;
+    double               phi_c[nqc * nb];       // [q][e]
+    double               RTk[nqc * DIM * nb];   // [q, s][e]
+    double               phi_f[Fq * nb];        // [fq][e]
+    double               RTr[Fq * nb];          // [fq][e]
+    double               RQk[nqc * DIM * Ft];   // [q, s][t]
+    double               RQr[Fq * Ft];          // [fq][t]
+    double               xi[Dm::nqf * Dm::nf];  // [qf][m]
+  };
+
   struct Ws3Off
   {
     // dead once Y is formed; the trace-row arrays below overlay them
@@ -94,7 +114,7 @@ namespace ddhdg
 
   template <int DIM, int K>
   __global__ void __launch_bounds__(Condense3MaxWPB * 32, 1)
-  condense3_kernel(const KParams P)
+  condense3_kernel(const KParams P, const __grid_constant__ CTab<DIM, K> C)
   {
     using Dm            = Dims<DIM, K>;
     constexpr int nb    = Dm::nb;
@@ -156,12 +176,14 @@ namespace ddhdg
     const bool   phi_mode = thermo || P.phi_linearize;
     const double ds       = (P.jfix & 1) ? -1. : 1.;
     const int    flux     = P.flux;
-    int          cmp[3]   = {P.comps[0], P.comps[1], P.comps[2]};
+    // enabled component c -> block index, two bits each (no local memory)
+    const int  cpk    = (P.comps[0] & 3) | ((P.comps[1] & 3) << 2) | ((P.comps[2] & 3) << 4);
+    const auto cmp_of = [cpk](int c) { return (cpk >> (2 * c)) & 3; };
     bool         nen = false, pen = false;
     for (int c = 0; c < ncomp; ++c)
       {
-        nen |= cmp[c] == 1;
-        pen |= cmp[c] == 2;
+        nen |= cmp_of(c) == 1;
+        pen |= cmp_of(c) == 2;
       }
     const int wpb = blockDim.x >> 5;
 
@@ -309,7 +331,7 @@ namespace ddhdg
         for (int i = lane; i < ncomp * DIM * nqc; i += 32)
           {
             const int     ce = i / (DIM * nqc);
-            const int     b  = cmp[ce];
+            const int     b  = cmp_of(ce);
             const int     s  = (i / nqc) % DIM;
             const int     q  = i % nqc;
             const double *cS = coef + (b * (DIM + 1) + DIM) * nb;
@@ -325,7 +347,7 @@ namespace ddhdg
         for (int i = lane; i < ncomp * Fq; i += 32)
           {
             const int     ce = i / Fq;
-            const int     b  = cmp[ce];
+            const int     b  = cmp_of(ce);
             const int     fq = i % Fq;
             const int     f = fq / nqf, qf = fq % nqf;
             const double *cS = coef + (b * (DIM + 1) + DIM) * nb;
@@ -467,7 +489,7 @@ namespace ddhdg
         // ------------------------------------------ residual coefficients
         for (int i = lane; i < ncomp * nqc; i += 32)
           {
-            const int    ce = i / nqc, q = i % nqc, b = cmp[ce];
+            const int    ce = i / nqc, q = i % nqc, b = cmp_of(ce);
             const double n0 = c0[nqc + q], p0 = c0[2 * nqc + q];
             double       v0, v1[DIM];
             if (b == 0)
@@ -488,7 +510,7 @@ namespace ddhdg
               }
             for (int cp = 0; cp < ncomp; ++cp)
               {
-                const double k_ = ka[(b * 3 + cmp[cp]) * nqc + q];
+                const double k_ = ka[(b * 3 + cmp_of(cp)) * nqc + q];
 #pragma unroll
                 for (int s = 0; s < DIM; ++s)
                   v1[s] -= k_ * Wrc[(cp * DIM + s) * nqc + q];
@@ -500,7 +522,7 @@ namespace ddhdg
           }
         for (int i = lane; i < ncomp * Fq; i += 32)
           {
-            const int    ce = i / Fq, fq = i % Fq, b = cmp[ce];
+            const int    ce = i / Fq, fq = i % Fq, b = cmp_of(ce);
             const double E0n = W0n[fq];
             const bool   cellside = (flux == 0) || (flux == 2 && E0n > 0.);
             const double tb_ = taus[(fq / nqf) * 3 + b];
@@ -517,13 +539,13 @@ namespace ddhdg
                 v                 = -tb_ * tb0 - Jf + tb_ * cb0;
               }
             for (int cp = 0; cp < ncomp; ++cp)
-              v -= rh[(b * 3 + cmp[cp]) * Fq + fq] * Wrf[cp * Fq + fq];
+              v -= rh[(b * 3 + cmp_of(cp)) * Fq + fq] * Wrf[cp * Fq + fq];
             rf[ce * Fq + fq] = v;
           }
         for (int t = lane; t < Nt; t += 32)
           {
             const int f = t / (ncomp * nf), ce = (t / nf) % ncomp, m = t % nf;
-            const int b = cmp[ce];
+            const int b = cmp_of(ce);
             double    g = 0., fl = 0.;
             if (bcs[f * 3 + b] == 1.)
               {
@@ -550,7 +572,7 @@ namespace ddhdg
         const bool act = lane < Ns;
         const int  ci  = act ? lane / nb : 0;
         const int  a   = act ? lane % nb : 0;
-        const int  bi  = cmp[ci];
+        const int  bi  = cmp_of(ci);
         if (act)
           {
             // residual column
@@ -575,14 +597,14 @@ namespace ddhdg
             // trace columns, one trial component at a time
             for (int cj = 0; cj < ncomp; ++cj)
               {
-                const int     pr  = bi * 3 + cmp[cj];
+                const int     pr  = bi * 3 + cmp_of(cj);
                 const double *kap = ka + pr * nqc;
                 const double *rhp = rh + pr * Fq;
                 double        acc[Ft];
 #pragma unroll
                 for (int t = 0; t < Ft; ++t)
                   acc[t] = 0.;
-#pragma unroll 1
+#pragma unroll
                 for (int q = 0; q < nqc; ++q)
                   {
                     const double kq = kap[q];
@@ -592,16 +614,16 @@ namespace ddhdg
                         const double w = kq * TLg[(q * DIM + s) * nb + a];
 #pragma unroll
                         for (int t = 0; t < Ft; ++t)
-                          acc[t] -= w * RQk[(q * DIM + s) * Ft + t];
+                          acc[t] -= w * C.RQk[(q * DIM + s) * Ft + t];
                       }
                   }
-#pragma unroll 1
+#pragma unroll
                 for (int fq = 0; fq < Fq; ++fq)
                   {
                     const double w = rhp[fq] * TLf[fq * nb + a];
 #pragma unroll
                     for (int t = 0; t < Ft; ++t)
-                      acc[t] -= w * RQr[fq * Ft + t];
+                      acc[t] -= w * C.RQr[fq * Ft + t];
                   }
                 if (cj == ci)
                   {
@@ -614,7 +636,7 @@ namespace ddhdg
                           const double w  = ctc[bi * Fq + fq] * TLf[fq * nb + a];
 #pragma unroll
                           for (int m = 0; m < nf; ++m)
-                            acc[f * nf + m] += w * xi[qf * nf + m];
+                            acc[f * nf + m] += w * C.xi[qf * nf + m];
                         }
                   }
 #pragma unroll
@@ -637,7 +659,7 @@ namespace ddhdg
                             for (int qf = 0; qf < nqf; ++qf)
                               {
                                 const int fq = f * nqf + qf;
-                                d += ctd[bi * Fq + fq] * TLf[fq * nb + a] * xi[qf * nf + m];
+                                d += ctd[bi * Fq + fq] * TLf[fq * nb + a] * C.xi[qf * nf + m];
                               }
                           R[lane * ldr + 1 + Nt + (f * ncomp + cj) * nf + m] = d;
                         }
@@ -654,12 +676,10 @@ namespace ddhdg
           srow[j] = (lane >= Ns && lane == j) ? 1. : 0.;
         if (act)
           {
-#pragma unroll
-            for (int cj = 0; cj < 3; ++cj)
+#pragma unroll 1
+            for (int cj = 0; cj < ncomp; ++cj)
               {
-                if (cj >= ncomp)
-                  break;
-                const int     pr  = bi * 3 + cmp[cj];
+                const int     pr  = bi * 3 + cmp_of(cj);
                 const double *alp = al + pr * nqc;
                 const double *kap = ka + pr * nqc;
                 const double *bep = be + pr * nqc * DIM;
@@ -669,7 +689,7 @@ namespace ddhdg
 #pragma unroll
                 for (int e = 0; e < nb; ++e)
                   acc[e] = 0.;
-#pragma unroll 1
+#pragma unroll
                 for (int q = 0; q < nqc; ++q)
                   {
                     double lt = alp[q] * TLc[q * nb + a];
@@ -684,27 +704,29 @@ namespace ddhdg
 #pragma unroll
                     for (int e = 0; e < nb; ++e)
                       {
-                        double v = lt * phi_c[q * nb + e];
+                        acc[e] += lt * C.phi_c[q * nb + e];
 #pragma unroll
                         for (int s = 0; s < DIM; ++s)
-                          v += kt[s] * RTk[(q * DIM + s) * nb + e];
-                        acc[e] += v;
+                          acc[e] += kt[s] * C.RTk[(q * DIM + s) * nb + e];
                       }
                   }
-#pragma unroll 1
+#pragma unroll
                 for (int fq = 0; fq < Fq; ++fq)
                   {
                     const double tf = TLf[fq * nb + a];
                     const double g_ = gap[fq] * tf, r_ = rhp[fq] * tf;
 #pragma unroll
                     for (int e = 0; e < nb; ++e)
-                      acc[e] += g_ * phi_f[fq * nb + e] + r_ * RTr[fq * nb + e];
+                      acc[e] += g_ * C.phi_f[fq * nb + e] + r_ * C.RTr[fq * nb + e];
                   }
+                // block cj of the row (selects: no dynamic register index)
 #pragma unroll
-                for (int e = 0; e < nb; ++e)
-                  srow[cj * nb + e] = acc[e];
+                for (int k = 0; k < NSMAX; ++k)
+                  if (k / nb == cj)
+                    srow[k] = acc[k % nb];
               }
           }
+        // ---------------------------------------- Gauss-Jordan inverse
         // Row equilibration: S' = D S with D = diag(1/max|row|).  The sweep
         // below inverts S'; S^-1 = S'^-1 D, so column k of the inverse is
         // scaled by the factor of row p_k before it multiplies R.
@@ -725,34 +747,45 @@ namespace ddhdg
         // at step j and NSMAX steps bring every column back to its place.
         // Afterwards lane p_j holds row j of S'^-1, whose column k belongs to
         // equation p_k.
-        bool used  = lane >= NSMAX;
-        int  mypos = 0;
-        bool sing  = false;
+        // Pivot choice: one warp max-reduction of a 32-bit key made of the
+        // high word of |S'_ij| (sign, exponent and 20 mantissa bits) with the
+        // low 5 bits replaced by 31 - lane: the pivot is within 2^-15 of the
+        // largest candidate, ties go to the lowest lane.  The pivot row is
+        // broadcast through shared memory (the coefficient block, dead here).
+        static_assert(NSMAX < 32, "key 0 marks used lanes");
+        double *prow  = coef;
+        bool    used  = lane >= NSMAX;
+        int     mypos = 0;
+        bool    sing  = false;
 #pragma unroll 1
         for (int j = 0; j < NSMAX; ++j)
           {
-            double best = used ? -1. : fabs(srow[0]);
-            int    bl   = lane;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
+            unsigned key = 0u;
+            if (!used)
               {
-                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                const int    oi = __shfl_xor_sync(0xffffffffu, bl, o);
-                if (ob > best || (ob == best && oi < bl))
-                  {
-                    best = ob;
-                    bl   = oi;
-                  }
+                const unsigned hi =
+                  (unsigned)((unsigned long long)__double_as_longlong(fabs(srow[0])) >> 32);
+                key = (hi & ~31u) | (31u - (unsigned)lane);
               }
-            sing |= !(best > 0.) || !isfinite(best);
-            const double pj = __shfl_sync(0xffffffffu, srow[0], bl);
+            const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+            const int      bl   = 31 - (int)(kmax & 31u);
+            const bool     me   = lane == bl;
+            if (me)
+              {
+#pragma unroll
+                for (int k = 0; k < NSMAX; k += 2)
+                  reinterpret_cast<double2 *>(prow)[k / 2] =
+                    make_double2(srow[k], k + 1 < NSMAX ? srow[k + 1] : 0.);
+              }
+            __syncwarp();
+            const double pj = prow[0];
+            sing |= kmax < 32u || !isfinite(pj);
             const double hr = (pj != 0.) ? 1. / pj : 0.;
-            const bool   me = lane == bl;
             const double l  = srow[0] * hr;
 #pragma unroll
             for (int k = 1; k < NSMAX; ++k)
               {
-                const double pk = __shfl_sync(0xffffffffu, srow[k], bl);
+                const double pk = prow[k];
                 srow[k - 1]     = me ? -pk * hr : srow[k] - l * pk;
               }
             srow[NSMAX - 1] = me ? hr : l;
@@ -763,6 +796,7 @@ namespace ddhdg
               }
             if (lane == 0)
               piv3[warp][j] = bl;
+            __syncwarp();
           }
         if (sing && lane == 0)
           atomicExch(P.status, 3);
@@ -863,7 +897,7 @@ namespace ddhdg
         for (int i = lane; i < Nt; i += 32)
           {
             const int fi = i / (ncomp * nf), ci2 = (i / nf) % ncomp, mi = i % nf;
-            const int b  = cmp[ci2];
+            const int b  = cmp_of(ci2);
             double    z  = 0.;
 #pragma unroll
             for (int qf = 0; qf < nqf; ++qf)
@@ -875,7 +909,7 @@ namespace ddhdg
                 z += w * rhsf[b * Fq + fq];
                 for (int cp = 0; cp < ncomp; ++cp)
                   {
-                    const double tw = w * tcW[(b * 3 + cmp[cp]) * Fq + fq];
+                    const double tw = w * tcW[(b * 3 + cmp_of(cp)) * Fq + fq];
                     rA[(i * 3 + cp) * nqf + qf] = tw;
                     z += tw * Hs[cp * Fq + fq];
                   }
