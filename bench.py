@@ -42,6 +42,55 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def flops_per_cell(dim, k, ncomp=3):
+    """Algorithmic FP64 flops of one cell's assembly + condensation (2 per
+    FMA): S and R assembly from the quadrature contractions, the inverse of
+    S, Y = S^-1 [residual | trace columns], the reduced trace operator T and
+    tt = T Y_t + tc_W Q_t."""
+    nb = (k + 1) ** dim
+    nf = (k + 1) ** (dim - 1)
+    F = 2 * dim
+    nqc, nqf = nb, nf
+    Fq, Ft = F * nqf, F * nf
+    Nt = F * ncomp * nf
+    Ns = ncomp * nb
+    fma = (Ns * Ns * (nqc * (1 + dim) + 2 * Fq)            # S
+           + Ns * ncomp * Ft * (nqc * dim + Fq)            # R, trace columns
+           + Ns * (nqc * (1 + dim) + Fq)                   # R, residual column
+           + Ns ** 3                                       # S^-1
+           + Ns * Ns * (1 + Nt)                            # Y
+           + Nt * Ns * 2 * nqf                             # T
+           + Nt * Nt * Ns + Nt * Nt * nqf)                 # tt
+    return 2 * fma
+
+
+def fp64_peak_tflops(dev):
+    """cuBLAS DGEMM 8192^3 throughput on this GPU (the FP64 ceiling)."""
+    import torch
+
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        c = a @ b
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        c = a @ b
+    e1.record()
+    torch.cuda.synchronize()
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 3 * 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+
+# DRAM bytes (read + write) of one condense launch per cell, from the ncu
+# capture summarised in profiles/condense3_2d_k2.md (16 384 cells: 14.8 MB
+# read + 260.1 MB written), scaled to a launch by the cells it processes
+TRAFFIC_BYTES_PER_CELL = 16779
+
+
 def bytes_per_cell(dim, k, ncomp=3):
     nb = (k + 1) ** dim
     nf = (k + 1) ** (dim - 1)
@@ -164,8 +213,8 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells-per-side", type=int, default=WORKLOAD["m"],
@@ -294,11 +343,14 @@ def main():
     e2e_ms = float(t2.item()) / args.steps
     e2e_value = world * nc / (e2e_ms * 1e-3)
 
+    fp64_peak = fp64_peak_tflops(dev)
     if rank == 0:
         hbm_peak, peak_kind = peaks()
         bc, br = bytes_per_cell(WORKLOAD["dim"], WORKLOAD["k"])
+        fc = flops_per_cell(WORKLOAD["dim"], WORKLOAD["k"])
         cond_avg = float(np.mean(cond_ms))
-        achieved = bc * nc / (cond_avg * 1e-3) / 1e9
+        achieved = fc * nc / (cond_avg * 1e-3) / 1e12
+        hbm_achieved = bc * nc / (cond_avg * 1e-3) / 1e9
         line = {
             "metric": "HDG cells condensed/s (assemble+condense+reconstruct)",
             "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
@@ -309,10 +361,15 @@ def main():
                        "parallelism": f"replicas x{world}",
                        "l2": "per-step traffic (>1.2 GB) exceeds the 126 MB L2"},
             "stages_ms": {"condense": cond_avg, "reconstruct": float(np.mean(rec_ms))},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": None,
-                         "kernel": "condense_kernel<2,2>", "peak_source": peak_kind,
-                         "algorithmic_bytes_per_cell": bc},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp64_peak,
+                         "traffic": (TRAFFIC_BYTES_PER_CELL * nc) if TRAFFIC_BYTES_PER_CELL else None,
+                         "kernel": "condense3_kernel<2,2>",
+                         "peak_source": "cuBLAS DGEMM 8192^3 timed in this run",
+                         "algorithmic_flops_per_cell": fc,
+                         "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                                 "frac": hbm_achieved / hbm_peak, "peak_source": peak_kind,
+                                 "algorithmic_bytes_per_cell": bc}},
             "e2e": {"value": e2e_value, "unit": "cells/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": 2 * args.steps,
