@@ -597,6 +597,26 @@ namespace
       }
   }
 
+  // scale row i of a CSR system (values and rhs) by 1 / max_j |a_ij|
+  __global__ void
+  row_equilibrate_kernel(int64_t n, const int32_t *rowptr, double *val, double *rhs)
+  {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+      {
+        double mx = 0.;
+        for (int32_t k = rowptr[i]; k < rowptr[i + 1]; ++k)
+          mx = fmax(mx, fabs(val[k]));
+        if (mx > 0.)
+          {
+            const double sc = 1. / mx;
+            for (int32_t k = rowptr[i]; k < rowptr[i + 1]; ++k)
+              val[k] *= sc;
+            rhs[i] *= sc;
+          }
+      }
+  }
+
   __global__ void
   gather_kernel(int64_t n, const int32_t *map, const double *src, double *dst)
   {
@@ -1248,10 +1268,15 @@ ddhdg_solve_trace(ddhdg_ctx *c, const double *csr, const double *grhs, double *x
   gather_kernel<<<grid_for(c, m.nnz, 256), 256, 0, s>>>(m.nnz, m.pmap.p, csr, m.pval.p);
   gather_kernel<<<grid_for(c, m.ndofs, 256), 256, 0, s>>>(m.ndofs, m.d_perm.p, grhs, m.pb.p);
   CK(cudaGetLastError());
+  // Row equilibration: the potential rows are ~1e19 next to unit Dirichlet
+  // identity rows, and Householder QR is only normwise backward stable, so
+  // every row is scaled to max |a_ij| = 1 before the factorisation.
+  row_equilibrate_kernel<<<grid_for(c, m.ndofs, 128), 128, 0, s>>>(m.ndofs, m.prow.p, m.pval.p, m.pb.p);
+  CK(cudaGetLastError());
   int sing = -1;
   const cusolverStatus_t st = cusolverSpDcsrlsvqr(
     c->sp, (int)m.ndofs, (int)m.nnz, c->descr, m.pval.p, m.prow.p, m.pcol.p, m.pb.p,
-    1e-14, 0, m.px.p, &sing);
+    0.0, 0, m.px.p, &sing); // tol 0: only an exactly zero R diagonal counts as singular
   if (st != CUSOLVER_STATUS_SUCCESS)
     return fail(DDHDG_SOLVER_ERROR, "cusolverSpDcsrlsvqr failed with status " + std::to_string((int)st));
   if (sing >= 0)

@@ -1,0 +1,131 @@
+"""Whole Newton solves on the GPU (ddhdg_newton: assembly + condensation,
+CSR scatter, the global trace solve, reconstruction, norms and damping on
+the device) against the oracle's Newton loop (src/np_solver.cpp:1452-1561)
+on the same problems."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from ddhdg_b200.problem import Component
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _npsolver():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    from ddhdg_b200.solver import NPSolver
+
+    return NPSolver
+
+
+def _oracle_from(g, pb, prm, adim):
+    o = O.OracleSolver(pb, prm, adim)
+    o.cell_state[:] = g.get_cell_state()
+    o.trace_state[:] = g.get_trace_state()
+    return o
+
+
+def _field_rel_err(a_cell, b_cell, a_trace, b_trace, oracle):
+    """Largest relative difference per component block (V, n, p), cell and
+    trace coefficients, against the block's largest magnitude."""
+    err = 0.0
+    d, nb = oracle.dim, oracle.nb
+    for c in range(3):
+        ia = slice(c * (d + 1) * nb, (c + 1) * (d + 1) * nb)
+        for a, b in ((a_cell[:, ia], b_cell[:, ia]), (a_trace[:, c], b_trace[:, c])):
+            scale = max(np.abs(b).max(), 1e-300)
+            err = max(err, float(np.abs(a - b).max() / scale))
+    return err
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_linear_potential_on_gpu(dim):
+    """tests/linear_potential.cpp:159-184 through the GPU Newton loop:
+    at most 3 iterations and L2 error below 1e-10."""
+    NPSolver = _npsolver()
+    pb, prm, adim = cases.linear_potential(dim, max_it=10)
+    g = NPSolver(pb, prm, adim)
+    g.set_component(Component.n, 0.0)
+    g.set_component(Component.p, 0.0)
+    res = g.run()
+    assert res.converged and res.iterations <= 3
+    o = _oracle_from(g, pb, prm, adim)
+    assert o.l2_error(Component.V, "x") < 1e-10
+    assert o.l2_error(Component.n, 0.0) < 1e-10
+    assert o.l2_error(Component.p, 0.0) < 1e-10
+
+
+@pytest.mark.parametrize("dim", [1, 2])
+def test_neumann_linear_on_gpu(dim):
+    """tests/neumann_boundary_conditions.cpp:160-187 through the GPU loop."""
+    NPSolver = _npsolver()
+    pb, prm, adim = cases.neumann_linear(dim)
+    g = NPSolver(pb, prm, adim)
+    g.set_component(Component.n, 0.0)
+    g.set_component(Component.p, 0.0)
+    res = g.run()
+    assert res.converged and res.iterations <= 3
+    o = _oracle_from(g, pb, prm, adim)
+    for c, f in ((Component.V, "x"), (Component.n, 0.0), (Component.p, 0.0)):
+        assert o.l2_error(c, f) < 1e-10
+
+
+def test_diode_config1_newton_matches_oracle():
+    """2D diode, 32x32 quads, degree 1, zero bias, Newton from thermodynamic
+    equilibrium, plain FP64: the final V, n, p fields match the oracle's
+    to 1e-10 relative.  The consistent Jacobian is switched on: with the
+    reference's E-coupling sign in the cell drift block
+    (include/assembling_methods.template.h:497-498, 520-521 against the
+    residual's Jn/Jp at 656-673) this Newton iteration diverges on the
+    CPU as well."""
+    NPSolver = _npsolver()
+    pb, prm, adim = cases.diode(dim=2, m=32, k=1)
+    prm.consistent_drift_jacobian = True
+    prm.consistent_recombination_jacobian = True
+    g = NPSolver(pb, prm, adim)
+    o = O.OracleSolver(pb, prm, adim)
+    # same first guess on both sides: the oracle's equilibrium start
+    o.compute_local_charge_neutrality()
+    g.set_state(o.cell_state, o.trace_state)
+    rg = g.private_run(1e-10, 1e-10, 50, thermo=True)
+    ro = o.private_run(1e-10, 1e-10, 50, thermo=True)
+    assert rg.converged and ro.converged
+    assert rg.iterations == ro.iterations
+    assert _field_rel_err(g.get_cell_state(), o.cell_state, g.get_trace_state(), o.trace_state, o) < 1e-10
+    # densities from the equilibrium potential, then the zero-bias solve
+    o.project_quasi_fermi(1)
+    o.project_quasi_fermi(2)
+    g.set_state(o.cell_state, o.trace_state)
+    rg = g.run()
+    ro = o.run()
+    assert rg.converged and ro.converged
+    assert rg.iterations == ro.iterations
+    assert _field_rel_err(g.get_cell_state(), o.cell_state, g.get_trace_state(), o.trace_state, o) < 1e-10
+
+
+def test_diode_forward_bias_newton_iterates_match_oracle():
+    """A forward-biased diode (0.3 V) from the equilibrium state: several
+    Newton iterations with the consistent Jacobian; the GPU after each
+    iteration count matches the oracle's iterate."""
+    NPSolver = _npsolver()
+    pb, prm, adim = cases.diode(dim=2, m=16, k=1, bias=0.3)
+    prm.consistent_drift_jacobian = True
+    prm.consistent_recombination_jacobian = True
+    o = O.OracleSolver(pb, prm, adim)
+    o.compute_local_charge_neutrality()
+    o.private_run(1e-10, 1e-10, 50, thermo=True)
+    o.project_quasi_fermi(1)
+    o.project_quasi_fermi(2)
+    start_cell, start_trace = o.cell_state.copy(), o.trace_state.copy()
+    o.private_run(0.0, 0.0, 4, record=True)
+    hist = o.newton_history
+    g = NPSolver(pb, prm, adim)
+    for it in (1, 2, 4):
+        g.set_state(start_cell, start_trace)
+        g.private_run(0.0, 0.0, it)
+        ref_cell, ref_trace = hist[it - 1]
+        assert _field_rel_err(g.get_cell_state(), ref_cell, g.get_trace_state(), ref_trace, o) < 1e-10, it
