@@ -27,6 +27,7 @@ EXPORTS = [
     "ddhdg_solve_trace", "ddhdg_reconstruct", "ddhdg_newton", "ddhdg_last_timings",
     "ddhdg_project_cell", "ddhdg_project_trace", "ddhdg_project_density",
     "ddhdg_reference_points", "ddhdg_last_error", "ddhdg_assemble_condense_noalloc",
+    "ddhdg_solve_condensed",
 ]
 
 
@@ -88,6 +89,7 @@ def load(build_if_missing: bool = True):
     L.ddhdg_scatter.argtypes = [c_void_p] + [c_void_p] * 6 + [c_int, c_void_p]
     L.ddhdg_get_csr.argtypes = [c_void_p, c_int, P(c_void_p), P(c_void_p)]
     L.ddhdg_solve_trace.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]
+    L.ddhdg_solve_condensed.argtypes = [c_void_p] * 6 + [c_int, c_void_p]
     L.ddhdg_reconstruct.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]
     L.ddhdg_newton.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, c_int,
                                c_double, P(c_int), P(c_double), c_void_p]

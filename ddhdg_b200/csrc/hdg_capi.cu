@@ -24,6 +24,7 @@
 #include "hdg_condense.cuh"
 #include "hdg_condense3.cuh"
 #include "hdg_kernels.cuh"
+#include "hdg_ndsolve.cuh"
 #include "hdg_tables.h"
 
 using namespace ddhdg;
@@ -108,6 +109,7 @@ namespace
     DevBuf<uint8_t>       slots; // [ncells][F][F]
     DevBuf<double>        ycache, tt, rhs, dval, csr, grhs, x, dtrace, dcell;
     DevBuf<double>        rscratch; // per-CTA R blocks of the condense kernel, if needed
+    std::unique_ptr<NDSolver> nd;   // nested-dissection trace solver (built on first use)
     DevBuf<int32_t>       dflag;
     std::vector<int32_t>  perm; // nested-dissection order of the trace dofs
     DevBuf<int32_t>       d_perm, d_iperm, prow, pcol;
@@ -276,6 +278,7 @@ namespace
   {
     Mode &m = c->mode[thermo];
     set_mode_comps(c, thermo);
+    m.nd.reset();
     const int     F = c->F, nf = c->nf, nc = m.ncomp;
     const int64_t nfaces = c->nfaces;
     // neighbour faces of every face
@@ -853,6 +856,40 @@ namespace
   }
 
   int
+  grid_for(const ddhdg_ctx *c, int64_t work, int block);
+
+  // the context's nested-dissection trace solver for one mode (built on
+  // first use: symbolic phase on the host, fronts on the device)
+  int
+  nd_solver(ddhdg_ctx *c, Mode &m, NDSolver *&out)
+  {
+    if (!m.nd)
+      {
+        NDSolver::Mesh M;
+        M.dim = c->dim;
+        for (int a = 0; a < 3; ++a)
+          {
+            M.n[a]        = (a < c->dim) ? c->desc.n[a] : 1;
+            M.face_off[a] = c->face_off[a];
+            for (int b = 0; b < 3; ++b)
+              M.face_ext[a][b] = c->face_ext[a][b];
+          }
+        M.ncells = c->ncells;
+        M.nfaces = c->nfaces;
+        M.F      = c->F;
+        M.nd     = m.ncomp * c->nf;
+        std::unique_ptr<NDSolver> nd(new NDSolver);
+        std::string               err;
+        const int                 r = nd->build(M, err);
+        if (r)
+          return fail(r, err);
+        m.nd = std::move(nd);
+      }
+    out = m.nd.get();
+    return DDHDG_OK;
+  }
+
+  int
   grid_for(const ddhdg_ctx *c, int64_t work, int block)
   {
     int64_t g = (work + block - 1) / block;
@@ -1164,6 +1201,26 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
 }
 
 int
+ddhdg_solve_condensed(ddhdg_ctx *c, const double *tt, const double *rhs, const int32_t *dflag,
+                      const double *dval, double *x, int thermo, ddhdg_stream_t stream)
+{
+  if (!c || !tt || !rhs || !dflag || !dval || !x)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo = thermo ? 1 : 0;
+  int   r;
+  Mode &m = c->mode[thermo];
+  if (!m.built && (r = build_mode(c, thermo)))
+    return r;
+  NDSolver *nd = nullptr;
+  if ((r = nd_solver(c, m, nd)))
+    return r;
+  std::string err;
+  if ((r = nd->solve(tt, rhs, dflag, dval, m.Nt, x, (cudaStream_t)stream, c->sm_count, err)))
+    return fail(r, err);
+  return DDHDG_OK;
+}
+
+int
 ddhdg_reconstruct(ddhdg_ctx *c, const double *cell_state, const double *trace_state,
                   const double *update_trace, double *update_cell, int thermo,
                   ddhdg_stream_t stream)
@@ -1323,11 +1380,9 @@ ddhdg_newton(ddhdg_ctx *c, double *cell_state, double *trace_state, int thermo,
       if ((rc = ddhdg_assemble_condense(c, cell_state, trace_state, thermo, m.tt.p, m.rhs.p,
                                         m.dflag.p, m.dval.p, stream)))
         break;
-      if ((rc = ddhdg_scatter(c, m.tt.p, m.rhs.p, m.dflag.p, m.dval.p, m.csr.p, m.grhs.p,
-                              thermo, stream)))
-        break;
       CK(cudaEventRecord(ev[1], s));
-      if ((rc = ddhdg_solve_trace(c, m.csr.p, m.grhs.p, m.x.p, thermo, stream)))
+      if ((rc = ddhdg_solve_condensed(c, m.tt.p, m.rhs.p, m.dflag.p, m.dval.p, m.x.p, thermo,
+                                      stream)))
         break;
       expand_kernel<<<grid_for(c, ntr_d, 256), 256, 0, s>>>(
         c->nfaces, c->nf, m.ncomp, m.comps[0], m.comps[1], m.comps[2], m.x.p, m.dtrace.p);

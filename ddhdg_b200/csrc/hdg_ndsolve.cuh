@@ -1,0 +1,724 @@
+// Global trace solve of the HDG system on a structured mesh (sm_100a, FP64).
+//
+// The global trace matrix is the sum over cells of the condensed per-cell
+// blocks tt (copy_local_to_global, src/np_solver.cpp:1293-1322, with the
+// Dirichlet rows replaced by identity rows).  The reference factorises it
+// with UMFPACK (src/np_solver.cpp:1326-1354).  Here it is factorised
+// directly from the per-cell blocks by nested dissection: the cell grid is
+// bisected recursively (longest axis first) and every tree node is a dense
+// front over the trace dofs of the faces on its split plane (eliminated
+// there) and of the faces on its boundary (kept for the parent).
+//
+//   leaves    one front per cell: the cell's block tt, with the faces on the
+//             physical boundary eliminated (Dirichlet dofs are identity rows)
+//   upward    a node's front is the extend-add of its two children's Schur
+//             complements; LU with partial pivoting of the eliminated block,
+//             W = F_EE^-1 [F_EK | r_E], Schur update F_KK -= F_KE W
+//   downward  x_E = y_E - W x_K from the root to the leaves
+//
+// Fronts of one height and one shape are processed as one batch (cuBLAS
+// batched LU, triangular solves and GEMMs; cuSOLVER dense LU for the few
+// large fronts near the root).  Before the factorisation the rows are
+// equilibrated: row g is scaled by 1 / max |row g| over the cells sharing it.
+#pragma once
+
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ddhdg_b200.h"
+
+namespace ddhdg
+{
+  struct NDAsm
+  {
+    int64_t off;     // front of the node (doubles)
+    int64_t coff[2]; // fronts of the children
+    int64_t moff[2]; // extend-add maps of the children
+    int     cnF[2], cnE[2];
+  };
+
+  struct NDSol
+  {
+    int64_t off;  // front
+    int64_t doff; // dof list
+  };
+
+  // rows of the leaf fronts: max |tt[a][:]| per global dof (bit pattern of a
+  // non-negative double, so that an integer max is the double max)
+  __global__ void
+  nd_rowmax_kernel(int64_t ncells, int Nt, int nd, int F, const int64_t *cell_faces,
+                   const double *tt, unsigned long long *dmax)
+  {
+    const int64_t tot = ncells * Nt;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < tot;
+         idx += (int64_t)gridDim.x * blockDim.x)
+      {
+        const int64_t cell = idx / Nt;
+        const int     a    = (int)(idx % Nt);
+        const double *row  = tt + (cell * Nt + a) * (int64_t)Nt;
+        double        m    = 0.;
+        for (int b = 0; b < Nt; ++b)
+          m = fmax(m, fabs(row[b]));
+        const int64_t g = cell_faces[cell * F + a / nd] * nd + a % nd;
+        atomicMax(dmax + g, (unsigned long long)__double_as_longlong(m));
+      }
+  }
+
+  __global__ void
+  nd_rowscale_kernel(int64_t n, const unsigned long long *dmax, double *dscale)
+  {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+      {
+        const double m = __longlong_as_double((long long)dmax[i]);
+        dscale[i]      = (m > 0.) ? 1. / m : 1.;
+      }
+  }
+
+  // leaf fronts (Nt x (Nt+1), column-major, last column the rhs) from the
+  // condensed blocks; front order: faces on the physical boundary first
+  // (local face order), then the others
+  __global__ void
+  nd_leaf_kernel(int64_t ncells, int Nt, int nd, int F, const uint8_t *pmask,
+                 const int64_t *leaf_off, const int64_t *cell_faces, const double *tt,
+                 const double *rhs, const int32_t *dflag, const double *dval,
+                 const double *dscale, double *fronts)
+  {
+    for (int64_t cell = blockIdx.x; cell < ncells; cell += gridDim.x)
+      {
+        const unsigned msk = pmask[cell];
+        int            rank[6];
+        int            r = 0;
+        for (int f = 0; f < F; ++f)
+          if (msk & (1u << f))
+            rank[f] = r++;
+        for (int f = 0; f < F; ++f)
+          if (!(msk & (1u << f)))
+            rank[f] = r++;
+        double        *Fr = fronts + leaf_off[cell];
+        const double  *tc = tt + cell * (int64_t)Nt * Nt;
+        const int32_t *fl = dflag + cell * (int64_t)Nt;
+        for (int idx = threadIdx.x; idx < Nt * (Nt + 1); idx += blockDim.x)
+          {
+            const int     b  = idx / Nt, a = idx % Nt;
+            const int     pa = rank[a / nd] * nd + a % nd;
+            const int64_t g  = cell_faces[cell * F + a / nd] * nd + a % nd;
+            if (b < Nt)
+              {
+                const int pb = rank[b / nd] * nd + b % nd;
+                Fr[(int64_t)pb * Nt + pa] =
+                  fl[a] ? (a == b ? 1. : 0.) : tc[(int64_t)a * Nt + b] * dscale[g];
+              }
+            else
+              Fr[(int64_t)Nt * Nt + pa] = fl[a] ? dval[cell * Nt + a] : rhs[cell * Nt + a] * dscale[g];
+          }
+      }
+  }
+
+  // extend-add of the children's Schur complements (kept rows/columns and
+  // the rhs column) into the node's front; one CTA per node, the two
+  // children one after the other (they overlap on the split-plane block)
+  __global__ void
+  nd_assemble_kernel(int nF, const NDAsm *nodes, const int32_t *emap, double *fronts)
+  {
+    const NDAsm nd = nodes[blockIdx.x];
+    double     *Fv = fronts + nd.off;
+    for (int s = 0; s < 2; ++s)
+      {
+        const int      cnF = nd.cnF[s], cnE = nd.cnE[s], cnK = cnF - cnE;
+        const double  *Fc  = fronts + nd.coff[s];
+        const int32_t *map = emap + nd.moff[s];
+        const int64_t  tot = (int64_t)cnK * (cnK + 1);
+        for (int64_t idx = threadIdx.x; idx < tot; idx += blockDim.x)
+          {
+            const int    j  = (int)(idx / cnK), i = (int)(idx % cnK);
+            const double v  = Fc[(int64_t)(cnE + j) * cnF + cnE + i];
+            const int    pj = (j < cnK) ? map[j] : nF;
+            Fv[(int64_t)pj * nF + map[i]] += v;
+          }
+        __syncthreads();
+      }
+  }
+
+  // x_E = y_E - W x_K for every node of a batch; one CTA per node
+  __global__ void
+  nd_backsolve_kernel(int nF, int nE, const NDSol *nodes, const int32_t *fdofs,
+                      const double *fronts, double *x)
+  {
+    extern __shared__ double xk[];
+    const NDSol    n  = nodes[blockIdx.x];
+    const int      nK = nF - nE;
+    const int32_t *dl = fdofs + n.doff;
+    for (int k = threadIdx.x; k < nK; k += blockDim.x)
+      xk[k] = x[dl[nE + k]];
+    __syncthreads();
+    const double *Fv = fronts + n.off;
+    for (int i = threadIdx.x; i < nE; i += blockDim.x)
+      {
+        double v = Fv[(int64_t)nF * nF + i];
+        for (int k = 0; k < nK; ++k)
+          v -= Fv[(int64_t)(nE + k) * nF + i] * xk[k];
+        x[dl[i]] = v;
+      }
+  }
+
+  // -------------------------------------------------------------- host side
+  class NDSolver
+  {
+  public:
+    struct Mesh
+    {
+      int     dim            = 2;
+      int     n[3]           = {1, 1, 1};
+      int64_t face_off[3]    = {0, 0, 0};
+      int     face_ext[3][3] = {{1, 1, 1}, {1, 1, 1}, {1, 1, 1}};
+      int64_t ncells = 0, nfaces = 0;
+      int     F  = 4;
+      int     nd = 1; // trace dofs per face (enabled components x face nodes)
+    };
+
+    ~NDSolver() { release(); }
+
+    bool built() const { return built_; }
+
+    int64_t front_bytes() const { return front_total_ * (int64_t)sizeof(double); }
+
+    // symbolic phase on the host: tree, fronts, maps and batches
+    int
+    plan(const Mesh &M, std::string &err)
+    {
+      release();
+      M_ = M;
+      if (M.F > 6 || M.dim < 1 || M.dim > 3)
+        return bad(err, "unsupported mesh for the nested-dissection solve");
+      if (M.nfaces * (int64_t)M.nd > INT32_MAX)
+        return bad(err, "too many trace dofs for 32-bit dof lists");
+      cell_faces_.assign(M.ncells * M.F, 0);
+      for (int64_t c = 0; c < M.ncells; ++c)
+        for (int f = 0; f < M.F; ++f)
+          cell_faces_[c * M.F + f] = face_of_cell(c, f);
+      nodes_.clear();
+      int lo[3] = {0, 0, 0}, hi[3] = {M.n[0], M.dim > 1 ? M.n[1] : 1, M.dim > 2 ? M.n[2] : 1};
+      root_ = make_node(lo, hi);
+      // batches: by height, then by shape
+      int maxh = 0;
+      for (auto &nd : nodes_)
+        maxh = std::max(maxh, nd.height);
+      std::vector<std::vector<int>> by_h(maxh + 1);
+      for (int i = 0; i < (int)nodes_.size(); ++i)
+        by_h[nodes_[i].height].push_back(i);
+      batches_.clear();
+      for (int h = 0; h <= maxh; ++h)
+        {
+          auto &ids = by_h[h];
+          std::sort(ids.begin(), ids.end(), [this](int a, int b) {
+            const auto &A = nodes_[a], &B = nodes_[b];
+            if (A.nE != B.nE)
+              return A.nE < B.nE;
+            if (A.nK != B.nK)
+              return A.nK < B.nK;
+            return a < b;
+          });
+          for (size_t i = 0; i < ids.size();)
+            {
+              size_t j = i;
+              while (j < ids.size() && nodes_[ids[j]].nE == nodes_[ids[i]].nE &&
+                     nodes_[ids[j]].nK == nodes_[ids[i]].nK)
+                ++j;
+              Batch b;
+              b.height = h;
+              b.nE     = nodes_[ids[i]].nE;
+              b.nK     = nodes_[ids[i]].nK;
+              b.nodes.assign(ids.begin() + i, ids.begin() + j);
+              batches_.push_back(std::move(b));
+              i = j;
+            }
+        }
+      // front, pivot and dof offsets in batch order
+      int64_t off = 0, poff = 0, doff = 0;
+      for (auto &b : batches_)
+        {
+          const int64_t nF = b.nE + b.nK;
+          b.front_off      = off;
+          b.piv_off        = poff;
+          for (int id : b.nodes)
+            {
+              nodes_[id].off = off;
+              off += nF * (nF + 1);
+              nodes_[id].doff = doff;
+              doff += nF;
+            }
+          poff += (int64_t)b.nE * b.nodes.size();
+          b.front_end = off;
+        }
+      front_total_ = off;
+      piv_total_   = poff;
+      // dof lists and extend-add maps
+      fdofs_h_.assign(doff, 0);
+      for (auto &nd : nodes_)
+        std::copy(nd.dofs.begin(), nd.dofs.end(), fdofs_h_.begin() + nd.doff);
+      std::vector<int32_t> pos(M.nfaces * (int64_t)M.nd, -1);
+      emap_h_.clear();
+      for (auto &nd : nodes_)
+        {
+          if (nd.child[0] < 0)
+            continue;
+          for (int i = 0; i < (int)nd.dofs.size(); ++i)
+            pos[nd.dofs[i]] = i;
+          for (int s = 0; s < 2; ++s)
+            {
+              const auto &ch = nodes_[nd.child[s]];
+              nd.moff[s]     = (int64_t)emap_h_.size();
+              for (int k = ch.nE; k < (int)ch.dofs.size(); ++k)
+                {
+                  const int32_t p = pos[ch.dofs[k]];
+                  if (p < 0)
+                    return bad(err, "nested dissection: a kept dof is missing from the parent front");
+                  emap_h_.push_back(p);
+                }
+            }
+          for (int32_t g : nd.dofs)
+            pos[g] = -1;
+        }
+      // leaves
+      leaf_off_h_.assign(M.ncells, 0);
+      pmask_h_.assign(M.ncells, 0);
+      for (auto &nd : nodes_)
+        if (nd.cell >= 0)
+          {
+            leaf_off_h_[nd.cell] = nd.off;
+            pmask_h_[nd.cell]    = (uint8_t)nd.pmask;
+          }
+      // per-batch tables: extend-add, back substitution, pointer offsets
+      asm_h_.clear();
+      sol_h_.clear();
+      ptr_h_.clear();
+      max_nK_ = 0;
+      for (auto &b : batches_)
+        {
+          const int nF = b.nE + b.nK;
+          b.asm_off    = (int64_t)asm_h_.size();
+          b.sol_off    = (int64_t)sol_h_.size();
+          b.ptr_off    = (int64_t)ptr_h_.size();
+          for (int id : b.nodes)
+            {
+              const auto &nd = nodes_[id];
+              if (nd.child[0] >= 0)
+                {
+                  NDAsm a{};
+                  a.off = nd.off;
+                  for (int s = 0; s < 2; ++s)
+                    {
+                      const auto &ch = nodes_[nd.child[s]];
+                      a.coff[s]      = ch.off;
+                      a.moff[s]      = nd.moff[s];
+                      a.cnF[s]       = ch.nE + ch.nK;
+                      a.cnE[s]       = ch.nE;
+                    }
+                  asm_h_.push_back(a);
+                }
+              sol_h_.push_back(NDSol{nd.off, nd.doff});
+            }
+          // F_EE, [F_EK | r_E], F_KE, F_KK of every node, as offsets
+          for (int q = 0; q < 4; ++q)
+            for (int id : b.nodes)
+              {
+                const int64_t o = nodes_[id].off;
+                ptr_h_.push_back(q == 0   ? o
+                                 : q == 1 ? o + (int64_t)b.nE * nF
+                                 : q == 2 ? o + b.nE
+                                          : o + (int64_t)b.nE * nF + b.nE);
+              }
+          b.big   = b.nE >= 384 && b.nodes.size() <= 32;
+          max_nK_ = std::max(max_nK_, b.nK);
+        }
+      return DDHDG_OK;
+    }
+
+    // symbolic phase (plan) and the device buffers
+    int
+    build(const Mesh &M, std::string &err)
+    {
+      int r;
+      if ((r = plan(M, err)))
+        return r;
+      if ((r = dmalloc(d_fronts_, front_total_ * sizeof(double), err)) ||
+          (r = dmalloc(d_piv_, std::max<int64_t>(piv_total_, 1) * sizeof(int), err)))
+        return r;
+      // one info per node, plus a sink for the solves' parameter status
+      if ((r = dmalloc(d_info_, (nodes_.size() + 1) * sizeof(int), err)))
+        return r;
+      if ((r = upload(d_fdofs_, fdofs_h_, err)) || (r = upload(d_emap_, emap_h_, err)) ||
+          (r = upload(d_leaf_off_, leaf_off_h_, err)) || (r = upload(d_pmask_, pmask_h_, err)) ||
+          (r = upload(d_cell_faces_, cell_faces_, err)) || (r = upload(d_asm_, asm_h_, err)) ||
+          (r = upload(d_sol_, sol_h_, err)))
+        return r;
+      std::vector<double *> ptrs(ptr_h_.size());
+      for (size_t q = 0; q < ptr_h_.size(); ++q)
+        ptrs[q] = d_fronts_ + ptr_h_[q];
+      if ((r = upload(d_ptr_, ptrs, err)))
+        return r;
+      const int64_t ndofs = M.nfaces * (int64_t)M.nd;
+      if ((r = dmalloc(d_dmax_, ndofs * sizeof(unsigned long long), err)) ||
+          (r = dmalloc(d_dscale_, ndofs * sizeof(double), err)))
+        return r;
+      if (cublasCreate(&blas_) != CUBLAS_STATUS_SUCCESS)
+        return bad(err, "cublasCreate failed", DDHDG_SOLVER_ERROR);
+      if (cusolverDnCreate(&dn_) != CUSOLVER_STATUS_SUCCESS)
+        return bad(err, "cusolverDnCreate failed", DDHDG_SOLVER_ERROR);
+      int64_t big_ws = 0;
+      for (auto &b : batches_)
+        if (b.big)
+          for (int id : b.nodes)
+            {
+              int       lw = 0;
+              const int nF = b.nE + b.nK;
+              if (cusolverDnDgetrf_bufferSize(dn_, b.nE, b.nE, d_fronts_ + nodes_[id].off, nF, &lw) !=
+                  CUSOLVER_STATUS_SUCCESS)
+                return bad(err, "cusolverDnDgetrf_bufferSize failed", DDHDG_SOLVER_ERROR);
+              big_ws = std::max<int64_t>(big_ws, lw);
+            }
+      if ((r = dmalloc(d_work_, std::max<int64_t>(big_ws, 1) * sizeof(double), err)))
+        return r;
+      if (max_nK_ * sizeof(double) > 48 * 1024)
+        if (cudaFuncSetAttribute(nd_backsolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(max_nK_ * sizeof(double))) != cudaSuccess)
+          return bad(err, "front too large for the back substitution", DDHDG_SOLVER_ERROR);
+      nodes_info_ = (int)nodes_.size();
+      built_      = true;
+      return DDHDG_OK;
+    }
+
+    // numeric phase: x (global trace dofs) from the per-cell condensed blocks
+    int
+    solve(const double *tt, const double *rhs, const int32_t *dflag, const double *dval, int Nt,
+          double *x, cudaStream_t s, int sm_count, std::string &err)
+    {
+      if (!built_)
+        return bad(err, "nested-dissection solver not built");
+      const auto   &M     = M_;
+      const int64_t ndofs = M.nfaces * (int64_t)M.nd;
+      const int     grid  = sm_count * 8;
+      if (Nt != M.F * M.nd)
+        return bad(err, "trace block size does not match the solver");
+      cublasSetStream(blas_, s);
+      cusolverDnSetStream(dn_, s);
+      // row equilibration
+      if (cudaMemsetAsync(d_dmax_, 0, ndofs * sizeof(unsigned long long), s) != cudaSuccess)
+        return bad(err, "memset failed", DDHDG_CUDA_ERROR);
+      nd_rowmax_kernel<<<grid, 256, 0, s>>>(M.ncells, Nt, M.nd, M.F, d_cell_faces_, tt, d_dmax_);
+      nd_rowscale_kernel<<<grid, 256, 0, s>>>(ndofs, d_dmax_, d_dscale_);
+      // leaves
+      nd_leaf_kernel<<<grid, 256, 0, s>>>(M.ncells, Nt, M.nd, M.F, d_pmask_, d_leaf_off_,
+                                          d_cell_faces_, tt, rhs, dflag, dval, d_dscale_, d_fronts_);
+      if (cudaMemsetAsync(d_info_, 0, (nodes_info_ + 1) * sizeof(int), s) != cudaSuccess)
+        return bad(err, "memset failed", DDHDG_CUDA_ERROR);
+      // upward pass
+      int info_base = 0;
+      for (auto &b : batches_)
+        {
+          const int nF = b.nE + b.nK;
+          const int nb = (int)b.nodes.size();
+          if (b.height > 0)
+            {
+              if (cudaMemsetAsync(d_fronts_ + b.front_off, 0,
+                                  (b.front_end - b.front_off) * sizeof(double), s) != cudaSuccess)
+                return bad(err, "memset failed", DDHDG_CUDA_ERROR);
+              nd_assemble_kernel<<<nb, 256, 0, s>>>(nF, d_asm_ + b.asm_off, d_emap_, d_fronts_);
+            }
+          if (b.nE > 0)
+            {
+              double **pEE = d_ptr_ + b.ptr_off, **pEK = pEE + nb, **pKE = pEK + nb, **pKK = pKE + nb;
+              int     *piv = d_piv_ + b.piv_off;
+              int     *inf = d_info_ + info_base;
+              if (b.big)
+                {
+                  for (int q = 0; q < nb; ++q)
+                    {
+                      double *Fq = d_fronts_ + nodes_[b.nodes[q]].off;
+                      if (cusolverDnDgetrf(dn_, b.nE, b.nE, Fq, nF, d_work_, piv + (int64_t)q * b.nE,
+                                           inf + q) != CUSOLVER_STATUS_SUCCESS)
+                        return bad(err, "cusolverDnDgetrf failed", DDHDG_SOLVER_ERROR);
+                      if (cusolverDnDgetrs(dn_, CUBLAS_OP_N, b.nE, b.nK + 1, Fq, nF,
+                                           piv + (int64_t)q * b.nE, Fq + (int64_t)b.nE * nF, nF,
+                                           d_info_ + nodes_info_) != CUSOLVER_STATUS_SUCCESS)
+                        return bad(err, "cusolverDnDgetrs failed", DDHDG_SOLVER_ERROR);
+                    }
+                }
+              else
+                {
+                  if (cublasDgetrfBatched(blas_, b.nE, pEE, nF, piv, inf, nb) != CUBLAS_STATUS_SUCCESS)
+                    return bad(err, "cublasDgetrfBatched failed", DDHDG_SOLVER_ERROR);
+                  int hinfo = 0;
+                  if (cublasDgetrsBatched(blas_, CUBLAS_OP_N, b.nE, b.nK + 1, pEE, nF, piv, pEK, nF,
+                                          &hinfo, nb) != CUBLAS_STATUS_SUCCESS ||
+                      hinfo != 0)
+                    return bad(err, "cublasDgetrsBatched failed", DDHDG_SOLVER_ERROR);
+                }
+              if (b.nK > 0)
+                {
+                  const double mone = -1., one = 1.;
+                  if (b.big)
+                    {
+                      for (int q = 0; q < nb; ++q)
+                        {
+                          double *Fq = d_fronts_ + nodes_[b.nodes[q]].off;
+                          if (cublasDgemm(blas_, CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE, &mone,
+                                          Fq + b.nE, nF, Fq + (int64_t)b.nE * nF, nF, &one,
+                                          Fq + (int64_t)b.nE * nF + b.nE, nF) != CUBLAS_STATUS_SUCCESS)
+                            return bad(err, "cublasDgemm failed", DDHDG_SOLVER_ERROR);
+                        }
+                    }
+                  else if (cublasDgemmBatched(blas_, CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE,
+                                              &mone, pKE, nF, pEK, nF, &one, pKK, nF,
+                                              nb) != CUBLAS_STATUS_SUCCESS)
+                    return bad(err, "cublasDgemmBatched failed", DDHDG_SOLVER_ERROR);
+                }
+            }
+          info_base += nb;
+        }
+      // downward pass
+      for (auto it = batches_.rbegin(); it != batches_.rend(); ++it)
+        {
+          const auto &b = *it;
+          if (b.nE == 0)
+            continue;
+          const int nF = b.nE + b.nK;
+          nd_backsolve_kernel<<<(int)b.nodes.size(), 256, b.nK * sizeof(double), s>>>(
+            nF, b.nE, d_sol_ + b.sol_off, d_fdofs_, d_fronts_, x);
+        }
+      if (cudaGetLastError() != cudaSuccess)
+        return bad(err, "nested-dissection kernel launch failed", DDHDG_CUDA_ERROR);
+      // singular fronts
+      std::vector<int> info(nodes_info_);
+      if (cudaMemcpyAsync(info.data(), d_info_, nodes_info_ * sizeof(int), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        return bad(err, "nested-dissection solve failed", DDHDG_CUDA_ERROR);
+      for (int v : info)
+        if (v != 0)
+          return bad(err, "global trace matrix is singular (zero pivot in a front)", DDHDG_SOLVER_ERROR);
+      return DDHDG_OK;
+    }
+
+  private:
+    struct Node
+    {
+      int                  lo[3], hi[3];
+      int                  child[2] = {-1, -1};
+      int                  height   = 0;
+      int64_t              cell     = -1;
+      unsigned             pmask    = 0;
+      int                  nE = 0, nK = 0;
+      std::vector<int32_t> dofs; // [E..., K...]
+      int64_t              off = 0, doff = 0, moff[2] = {0, 0};
+    };
+    struct Batch
+    {
+      int              height = 0, nE = 0, nK = 0;
+      std::vector<int> nodes;
+      int64_t          front_off = 0, front_end = 0, piv_off = 0, asm_off = 0, sol_off = 0, ptr_off = 0;
+      bool             big = false;
+    };
+
+    static int
+    bad(std::string &err, const char *msg, int code = DDHDG_BAD_ARG)
+    {
+      err = msg;
+      return code;
+    }
+
+    int64_t
+    face_at(int a, const int co[3]) const
+    {
+      int64_t idx = 0, stride = 1;
+      for (int b = 0; b < M_.dim; ++b)
+        {
+          idx += co[b] * stride;
+          stride *= M_.face_ext[a][b];
+        }
+      return M_.face_off[a] + idx;
+    }
+
+    int64_t
+    face_of_cell(int64_t cell, int f) const
+    {
+      int       co[3];
+      const int n1 = M_.dim > 1 ? M_.n[1] : 1;
+      co[0]        = (int)(cell % M_.n[0]);
+      co[1]        = (int)((cell / M_.n[0]) % n1);
+      co[2]        = (int)(cell / ((int64_t)M_.n[0] * n1));
+      co[f / 2] += f % 2;
+      return face_at(f / 2, co);
+    }
+
+    // faces of axis a at face coordinate p, over the box's extent in the
+    // other axes, in increasing id order
+    void
+    plane_faces(int a, int p, const int lo[3], const int hi[3], std::vector<int64_t> &out) const
+    {
+      int co[3];
+      int l[3], h[3];
+      for (int b = 0; b < 3; ++b)
+        {
+          l[b] = (b == a) ? p : lo[b];
+          h[b] = (b == a) ? p + 1 : hi[b];
+        }
+      for (co[2] = l[2]; co[2] < h[2]; ++co[2])
+        for (co[1] = l[1]; co[1] < h[1]; ++co[1])
+          for (co[0] = l[0]; co[0] < h[0]; ++co[0])
+            out.push_back(face_at(a, co));
+    }
+
+    void
+    expand(const std::vector<int64_t> &faces, std::vector<int32_t> &dofs) const
+    {
+      for (int64_t f : faces)
+        for (int j = 0; j < M_.nd; ++j)
+          dofs.push_back((int32_t)(f * M_.nd + j));
+    }
+
+    int
+    make_node(const int lo[3], const int hi[3])
+    {
+      const int id = (int)nodes_.size();
+      nodes_.emplace_back();
+      for (int b = 0; b < 3; ++b)
+        {
+          nodes_[id].lo[b] = lo[b];
+          nodes_[id].hi[b] = hi[b];
+        }
+      const int ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+      if (ext[0] * ext[1] * ext[2] == 1)
+        {
+          // leaf: one cell; faces on the physical boundary first
+          const int     n1   = M_.dim > 1 ? M_.n[1] : 1;
+          const int64_t cell = lo[0] + (int64_t)M_.n[0] * (lo[1] + (int64_t)n1 * lo[2]);
+          std::vector<int64_t> E, K;
+          unsigned             msk = 0;
+          for (int f = 0; f < M_.F; ++f)
+            {
+              const int a = f / 2, p = (f % 2) ? hi[a] : lo[a];
+              if (p == 0 || p == M_.n[a])
+                msk |= 1u << f;
+            }
+          for (int f = 0; f < M_.F; ++f)
+            ((msk & (1u << f)) ? E : K).push_back(cell_faces_[cell * M_.F + f]);
+          auto &nd = nodes_[id];
+          nd.cell  = cell;
+          nd.pmask = msk;
+          expand(E, nd.dofs);
+          nd.nE = (int)nd.dofs.size();
+          expand(K, nd.dofs);
+          nd.nK     = (int)nd.dofs.size() - nd.nE;
+          nd.height = 0;
+          return id;
+        }
+      int s = 0;
+      for (int b = 1; b < M_.dim; ++b)
+        if (ext[b] > ext[s])
+          s = b;
+      const int mid   = lo[s] + ext[s] / 2;
+      int       hl[3] = {hi[0], hi[1], hi[2]}, lh[3] = {lo[0], lo[1], lo[2]};
+      hl[s]           = mid;
+      lh[s]           = mid;
+      const int c0    = make_node(lo, hl);
+      const int c1    = make_node(lh, hi);
+      std::vector<int64_t> E, K;
+      plane_faces(s, mid, lo, hi, E);
+      for (int a = 0; a < M_.dim; ++a)
+        {
+          if (lo[a] > 0)
+            plane_faces(a, lo[a], lo, hi, K);
+          if (hi[a] < M_.n[a])
+            plane_faces(a, hi[a], lo, hi, K);
+        }
+      std::sort(K.begin(), K.end());
+      auto &nd    = nodes_[id]; // after the recursion: nodes_ may have grown
+      nd.child[0] = c0;
+      nd.child[1] = c1;
+      expand(E, nd.dofs);
+      nd.nE = (int)nd.dofs.size();
+      expand(K, nd.dofs);
+      nd.nK     = (int)nd.dofs.size() - nd.nE;
+      nd.height = 1 + std::max(nodes_[c0].height, nodes_[c1].height);
+      return id;
+    }
+
+    template <typename T>
+    int
+    dmalloc(T *&p, size_t bytes, std::string &err)
+    {
+      if (cudaMalloc(reinterpret_cast<void **>(&p), std::max<size_t>(bytes, 16)) != cudaSuccess)
+        {
+          cudaGetLastError();
+          p   = nullptr;
+          err = "cudaMalloc of " + std::to_string(bytes) + " bytes for the trace solver failed";
+          return DDHDG_OOM;
+        }
+      allocs_.push_back(p);
+      return DDHDG_OK;
+    }
+
+    template <typename T>
+    int
+    upload(T *&p, const std::vector<T> &v, std::string &err)
+    {
+      int r = dmalloc(p, v.size() * sizeof(T), err);
+      if (r)
+        return r;
+      if (!v.empty() && cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bad(err, "upload failed", DDHDG_CUDA_ERROR);
+      return DDHDG_OK;
+    }
+
+    void
+    release()
+    {
+      for (void *p : allocs_)
+        cudaFree(p);
+      allocs_.clear();
+      if (blas_)
+        cublasDestroy(blas_);
+      if (dn_)
+        cusolverDnDestroy(dn_);
+      blas_  = nullptr;
+      dn_    = nullptr;
+      built_ = false;
+    }
+
+    Mesh                 M_;
+    std::vector<Node>    nodes_;
+    std::vector<Batch>   batches_;
+    std::vector<int64_t> cell_faces_;
+    int                  root_ = -1, nodes_info_ = 0, max_nK_ = 0;
+    int64_t              front_total_ = 0, piv_total_ = 0;
+    bool                 built_       = false;
+    // host copies of the plan (uploaded by build)
+    std::vector<int32_t> fdofs_h_, emap_h_;
+    std::vector<int64_t> leaf_off_h_, ptr_h_;
+    std::vector<uint8_t> pmask_h_;
+    std::vector<NDAsm>   asm_h_;
+    std::vector<NDSol>   sol_h_;
+    // device
+    std::vector<void *> allocs_;
+    double             *d_fronts_ = nullptr, *d_dscale_ = nullptr, *d_work_ = nullptr;
+    double            **d_ptr_    = nullptr;
+    int                *d_piv_ = nullptr, *d_info_ = nullptr;
+    int32_t            *d_fdofs_ = nullptr, *d_emap_ = nullptr;
+    int64_t            *d_leaf_off_ = nullptr, *d_cell_faces_ = nullptr;
+    uint8_t            *d_pmask_ = nullptr;
+    NDAsm              *d_asm_   = nullptr;
+    NDSol              *d_sol_   = nullptr;
+    unsigned long long *d_dmax_  = nullptr;
+    cublasHandle_t      blas_    = nullptr;
+    cusolverDnHandle_t  dn_      = nullptr;
+  };
+} // namespace ddhdg

@@ -193,6 +193,17 @@ int ddhdg_solve_trace(ddhdg_ctx *ctx, const double *csr_values,
                       const double *global_rhs, double *x, int thermo_eq,
                       ddhdg_stream_t stream);
 
+/* copy_local_to_global + solve_linear_problem (src/np_solver.cpp:1293-1354)
+ * in one call: x = A^-1 b for the global trace system assembled from the
+ * per-cell condensed blocks of ddhdg_assemble_condense (Dirichlet dofs take
+ * their projected values).  Nested-dissection multifrontal LU on the device;
+ * the first call on a context (and mode) builds the elimination tree and
+ * allocates the fronts.  x has n_trace_dofs entries in the restricted trace
+ * order. */
+int ddhdg_solve_condensed(ddhdg_ctx *ctx, const double *tt, const double *rhs,
+                          const int32_t *dflag, const double *dval, double *x,
+                          int thermo_eq, ddhdg_stream_t stream);
+
 /* assemble_system(true, thermo_eq): cell update from the full trace update
  * update_trace [nfaces][3][nf] (include/assembling_methods.template.h:
  * 2122-2160 and 2688-2697).  Uses the reconstruction data kept by the last
