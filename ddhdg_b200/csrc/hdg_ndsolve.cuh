@@ -122,32 +122,36 @@ namespace ddhdg
       }
   }
 
-  // extend-add of the children's Schur complements (kept rows/columns and
-  // the rhs column) into the node's front; one CTA per node, the two
-  // children one after the other (they overlap on the split-plane block)
+  // extend-add of child s's Schur complement (kept rows/columns and the rhs
+  // column) into the node's front: CTA (node, block of NDAsmCols child
+  // columns).  The two children are added by two launches, one after the
+  // other (they overlap on the split-plane block).
+  constexpr int NDAsmCols = 8;
+
   __global__ void
-  nd_assemble_kernel(int nF, const NDAsm *nodes, const int32_t *emap, double *fronts)
+  nd_assemble_kernel(int nF, int s, const NDAsm *nodes, const int32_t *emap, double *fronts)
   {
-    const NDAsm nd = nodes[blockIdx.x];
-    double     *Fv = fronts + nd.off;
-    for (int s = 0; s < 2; ++s)
+    const NDAsm    nd  = nodes[blockIdx.x];
+    const int      cnF = nd.cnF[s], cnE = nd.cnE[s], cnK = cnF - cnE;
+    const int      j0  = blockIdx.y * NDAsmCols;
+    if (j0 > cnK)
+      return;
+    double        *Fv  = fronts + nd.off;
+    const double  *Fc  = fronts + nd.coff[s];
+    const int32_t *map = emap + nd.moff[s];
+    const int      j1  = min(cnK + 1, j0 + NDAsmCols);
+    for (int j = j0; j < j1; ++j)
       {
-        const int      cnF = nd.cnF[s], cnE = nd.cnE[s], cnK = cnF - cnE;
-        const double  *Fc  = fronts + nd.coff[s];
-        const int32_t *map = emap + nd.moff[s];
-        const int64_t  tot = (int64_t)cnK * (cnK + 1);
-        for (int64_t idx = threadIdx.x; idx < tot; idx += blockDim.x)
-          {
-            const int    j  = (int)(idx / cnK), i = (int)(idx % cnK);
-            const double v  = Fc[(int64_t)(cnE + j) * cnF + cnE + i];
-            const int    pj = (j < cnK) ? map[j] : nF;
-            Fv[(int64_t)pj * nF + map[i]] += v;
-          }
-        __syncthreads();
+        const int     pj = (j < cnK) ? map[j] : nF;
+        const double *cj = Fc + (int64_t)(cnE + j) * cnF + cnE;
+        double       *vj = Fv + (int64_t)pj * nF;
+        for (int i = threadIdx.x; i < cnK; i += blockDim.x)
+          vj[map[i]] += cj[i];
       }
   }
 
-  // x_E = y_E - W x_K for every node of a batch; one CTA per node
+  // x_E = y_E - W x_K for every node of a batch; CTA (node, block of 256
+  // eliminated rows)
   __global__ void
   nd_backsolve_kernel(int nF, int nE, const NDSol *nodes, const int32_t *fdofs,
                       const double *fronts, double *x)
@@ -160,7 +164,8 @@ namespace ddhdg
       xk[k] = x[dl[nE + k]];
     __syncthreads();
     const double *Fv = fronts + n.off;
-    for (int i = threadIdx.x; i < nE; i += blockDim.x)
+    const int     i  = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i < nE)
       {
         double v = Fv[(int64_t)nF * nF + i];
         for (int k = 0; k < nK; ++k)
@@ -323,6 +328,8 @@ namespace ddhdg
                       a.cnE[s]       = ch.nE;
                     }
                   asm_h_.push_back(a);
+                  for (int s = 0; s < 2; ++s)
+                    b.maxc[s] = std::max(b.maxc[s], a.cnF[s] - a.cnE[s] + 1);
                 }
               sol_h_.push_back(NDSol{nd.off, nd.doff});
             }
@@ -431,7 +438,11 @@ namespace ddhdg
               if (cudaMemsetAsync(d_fronts_ + b.front_off, 0,
                                   (b.front_end - b.front_off) * sizeof(double), s) != cudaSuccess)
                 return bad(err, "memset failed", DDHDG_CUDA_ERROR);
-              nd_assemble_kernel<<<nb, 256, 0, s>>>(nF, d_asm_ + b.asm_off, d_emap_, d_fronts_);
+              for (int c = 0; c < 2; ++c)
+                {
+                  const dim3 g2(nb, (b.maxc[c] + NDAsmCols - 1) / NDAsmCols);
+                  nd_assemble_kernel<<<g2, 256, 0, s>>>(nF, c, d_asm_ + b.asm_off, d_emap_, d_fronts_);
+                }
             }
           if (b.nE > 0)
             {
@@ -491,8 +502,9 @@ namespace ddhdg
           if (b.nE == 0)
             continue;
           const int nF = b.nE + b.nK;
-          nd_backsolve_kernel<<<(int)b.nodes.size(), 256, b.nK * sizeof(double), s>>>(
-            nF, b.nE, d_sol_ + b.sol_off, d_fdofs_, d_fronts_, x);
+          const dim3 g2((unsigned)b.nodes.size(), (b.nE + 255) / 256);
+          nd_backsolve_kernel<<<g2, 256, b.nK * sizeof(double), s>>>(nF, b.nE, d_sol_ + b.sol_off,
+                                                                     d_fdofs_, d_fronts_, x);
         }
       if (cudaGetLastError() != cudaSuccess)
         return bad(err, "nested-dissection kernel launch failed", DDHDG_CUDA_ERROR);
@@ -525,7 +537,8 @@ namespace ddhdg
       int              height = 0, nE = 0, nK = 0;
       std::vector<int> nodes;
       int64_t          front_off = 0, front_end = 0, piv_off = 0, asm_off = 0, sol_off = 0, ptr_off = 0;
-      bool             big = false;
+      bool             big     = false;
+      int              maxc[2] = {0, 0}; // max child nK + 1 per extend-add pass
     };
 
     static int
