@@ -174,6 +174,53 @@ namespace ddhdg
       }
   }
 
+  // row permutation of a batch's LU factorisations: the sequential swaps of
+  // ipiv (1-based) turned into perm[i] = source row of row i; one thread per
+  // front
+  __global__ void
+  nd_pivperm_kernel(int nb, int nE, const int *ipiv, int *perm)
+  {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nb)
+      return;
+    const int *pv = ipiv + (int64_t)q * nE;
+    int       *pm = perm + (int64_t)q * nE;
+    for (int i = 0; i < nE; ++i)
+      pm[i] = i;
+    for (int j = 0; j < nE; ++j)
+      {
+        const int k = pv[j] - 1;
+        const int t = pm[j];
+        pm[j]       = pm[k];
+        pm[k]       = t;
+      }
+  }
+
+  // B = P B for the rows 0..nE-1 of the columns [nE, nF] of every front of a
+  // batch (the right-hand sides of F_EE W = [F_EK | r_E]), in place, one
+  // column at a time through shared memory; CTA (front, block of columns)
+  constexpr int NDPermCols = 8;
+
+  __global__ void
+  nd_rowperm_kernel(int nE, int nF, const NDSol *nodes, const int *perm, double *fronts)
+  {
+    extern __shared__ double col[];
+    const int64_t off = nodes[blockIdx.x].off;
+    const int    *pm  = perm + (int64_t)blockIdx.x * nE;
+    const int     c0  = blockIdx.y * NDPermCols;
+    const int     c1  = min(nF - nE + 1, c0 + NDPermCols);
+    for (int c = c0; c < c1; ++c)
+      {
+        double *B = fronts + off + (int64_t)(nE + c) * nF;
+        for (int i = threadIdx.x; i < nE; i += blockDim.x)
+          col[i] = B[i];
+        __syncthreads();
+        for (int i = threadIdx.x; i < nE; i += blockDim.x)
+          B[i] = col[pm[i]];
+        __syncthreads();
+      }
+  }
+
   // -------------------------------------------------------------- host side
   class NDSolver
   {
@@ -357,7 +404,8 @@ namespace ddhdg
       if ((r = plan(M, err)))
         return r;
       if ((r = dmalloc(d_fronts_, front_total_ * sizeof(double), err)) ||
-          (r = dmalloc(d_piv_, std::max<int64_t>(piv_total_, 1) * sizeof(int), err)))
+          (r = dmalloc(d_piv_, std::max<int64_t>(piv_total_, 1) * sizeof(int), err)) ||
+          (r = dmalloc(d_perm_, std::max<int64_t>(piv_total_, 1) * sizeof(int), err)))
         return r;
       // one info per node, plus a sink for the solves' parameter status
       if ((r = dmalloc(d_info_, (nodes_.size() + 1) * sizeof(int), err)))
@@ -394,6 +442,13 @@ namespace ddhdg
             }
       if ((r = dmalloc(d_work_, std::max<int64_t>(big_ws, 1) * sizeof(double), err)))
         return r;
+      int max_nE = 0;
+      for (auto &b : batches_)
+        max_nE = std::max(max_nE, b.nE);
+      if (max_nE * sizeof(double) > 48 * 1024)
+        if (cudaFuncSetAttribute(nd_rowperm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(max_nE * sizeof(double))) != cudaSuccess)
+          return bad(err, "front too large for the row permutation", DDHDG_SOLVER_ERROR);
       if (max_nK_ * sizeof(double) > 48 * 1024)
         if (cudaFuncSetAttribute(nd_backsolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(max_nK_ * sizeof(double))) != cudaSuccess)
@@ -457,22 +512,41 @@ namespace ddhdg
                       if (cusolverDnDgetrf(dn_, b.nE, b.nE, Fq, nF, d_work_, piv + (int64_t)q * b.nE,
                                            inf + q) != CUSOLVER_STATUS_SUCCESS)
                         return bad(err, "cusolverDnDgetrf failed", DDHDG_SOLVER_ERROR);
-                      if (cusolverDnDgetrs(dn_, CUBLAS_OP_N, b.nE, b.nK + 1, Fq, nF,
-                                           piv + (int64_t)q * b.nE, Fq + (int64_t)b.nE * nF, nF,
-                                           d_info_ + nodes_info_) != CUSOLVER_STATUS_SUCCESS)
-                        return bad(err, "cusolverDnDgetrs failed", DDHDG_SOLVER_ERROR);
                     }
                 }
-              else
+              else if (cublasDgetrfBatched(blas_, b.nE, pEE, nF, piv, inf, nb) != CUBLAS_STATUS_SUCCESS)
+                return bad(err, "cublasDgetrfBatched failed", DDHDG_SOLVER_ERROR);
+              // W = U^-1 L^-1 P [F_EK | r_E]: the row permutation by a
+              // coalesced in-place gather, then two triangular solves
+              int *perm = d_perm_ + b.piv_off;
+              nd_pivperm_kernel<<<(nb + 127) / 128, 128, 0, s>>>(nb, b.nE, piv, perm);
+              {
+                const dim3 g2(nb, (b.nK + 1 + NDPermCols - 1) / NDPermCols);
+                nd_rowperm_kernel<<<g2, 256, b.nE * sizeof(double), s>>>(b.nE, nF, d_sol_ + b.sol_off,
+                                                                         perm, d_fronts_);
+              }
+              const double one_ = 1.;
+              if (b.big)
                 {
-                  if (cublasDgetrfBatched(blas_, b.nE, pEE, nF, piv, inf, nb) != CUBLAS_STATUS_SUCCESS)
-                    return bad(err, "cublasDgetrfBatched failed", DDHDG_SOLVER_ERROR);
-                  int hinfo = 0;
-                  if (cublasDgetrsBatched(blas_, CUBLAS_OP_N, b.nE, b.nK + 1, pEE, nF, piv, pEK, nF,
-                                          &hinfo, nb) != CUBLAS_STATUS_SUCCESS ||
-                      hinfo != 0)
-                    return bad(err, "cublasDgetrsBatched failed", DDHDG_SOLVER_ERROR);
+                  for (int q = 0; q < nb; ++q)
+                    {
+                      double *Fq = d_fronts_ + nodes_[b.nodes[q]].off;
+                      if (cublasDtrsm(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                                      CUBLAS_DIAG_UNIT, b.nE, b.nK + 1, &one_, Fq, nF,
+                                      Fq + (int64_t)b.nE * nF, nF) != CUBLAS_STATUS_SUCCESS ||
+                          cublasDtrsm(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                                      CUBLAS_DIAG_NON_UNIT, b.nE, b.nK + 1, &one_, Fq, nF,
+                                      Fq + (int64_t)b.nE * nF, nF) != CUBLAS_STATUS_SUCCESS)
+                        return bad(err, "cublasDtrsm failed", DDHDG_SOLVER_ERROR);
+                    }
                 }
+              else if (cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                                          CUBLAS_DIAG_UNIT, b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF,
+                                          nb) != CUBLAS_STATUS_SUCCESS ||
+                       cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                                          CUBLAS_DIAG_NON_UNIT, b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF,
+                                          nb) != CUBLAS_STATUS_SUCCESS)
+                return bad(err, "cublasDtrsmBatched failed", DDHDG_SOLVER_ERROR);
               if (b.nK > 0)
                 {
                   const double mone = -1., one = 1.;
@@ -724,7 +798,7 @@ namespace ddhdg
     std::vector<void *> allocs_;
     double             *d_fronts_ = nullptr, *d_dscale_ = nullptr, *d_work_ = nullptr;
     double            **d_ptr_    = nullptr;
-    int                *d_piv_ = nullptr, *d_info_ = nullptr;
+    int                *d_piv_ = nullptr, *d_perm_ = nullptr, *d_info_ = nullptr;
     int32_t            *d_fdofs_ = nullptr, *d_emap_ = nullptr;
     int64_t            *d_leaf_off_ = nullptr, *d_cell_faces_ = nullptr;
     uint8_t            *d_pmask_ = nullptr;
