@@ -440,8 +440,22 @@ namespace ddhdg
                 return bad(err, "cusolverDnDgetrf_bufferSize failed", DDHDG_SOLVER_ERROR);
               big_ws = std::max<int64_t>(big_ws, lw);
             }
-      if ((r = dmalloc(d_work_, std::max<int64_t>(big_ws, 1) * sizeof(double), err)))
+      work_per_ = std::max<int64_t>(big_ws, 1);
+      if ((r = dmalloc(d_work_, NSide * work_per_ * sizeof(double), err)))
         return r;
+      if (cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) != cudaSuccess)
+        return bad(err, "cudaEventCreate failed", DDHDG_CUDA_ERROR);
+      for (int k = 0; k < NSide; ++k)
+        {
+          if (cudaStreamCreateWithFlags(&side_[k], cudaStreamNonBlocking) != cudaSuccess ||
+              cudaEventCreateWithFlags(&ev_join_[k], cudaEventDisableTiming) != cudaSuccess)
+            return bad(err, "cudaStreamCreate failed", DDHDG_CUDA_ERROR);
+          if (cublasCreate(&side_blas_[k]) != CUBLAS_STATUS_SUCCESS ||
+              cusolverDnCreate(&side_dn_[k]) != CUSOLVER_STATUS_SUCCESS)
+            return bad(err, "handle creation failed", DDHDG_SOLVER_ERROR);
+          cublasSetStream(side_blas_[k], side_[k]);
+          cusolverDnSetStream(side_dn_[k], side_[k]);
+        }
       int max_nE = 0;
       for (auto &b : batches_)
         max_nE = std::max(max_nE, b.nE);
@@ -506,15 +520,13 @@ namespace ddhdg
               int     *inf = d_info_ + info_base;
               if (b.big)
                 {
-                  for (int q = 0; q < nb; ++q)
-                    {
-                      double *Fq = d_fronts_ + nodes_[b.nodes[q]].off;
-                      if (cusolverDnDgetrf(dn_, b.nE, b.nE, Fq, nF, d_work_, piv + (int64_t)q * b.nE,
-                                           inf + q) != CUSOLVER_STATUS_SUCCESS)
-                        return bad(err, "cusolverDnDgetrf failed", DDHDG_SOLVER_ERROR);
-                    }
+                  int r;
+                  if ((r = big_batch(b, info_base, s, err)))
+                    return r;
+                  info_base += nb;
+                  continue;
                 }
-              else if (cublasDgetrfBatched(blas_, b.nE, pEE, nF, piv, inf, nb) != CUBLAS_STATUS_SUCCESS)
+              if (cublasDgetrfBatched(blas_, b.nE, pEE, nF, piv, inf, nb) != CUBLAS_STATUS_SUCCESS)
                 return bad(err, "cublasDgetrfBatched failed", DDHDG_SOLVER_ERROR);
               // W = U^-1 L^-1 P [F_EK | r_E]: the row permutation by a
               // coalesced in-place gather, then two triangular solves
@@ -526,44 +538,18 @@ namespace ddhdg
                                                                          perm, d_fronts_);
               }
               const double one_ = 1.;
-              if (b.big)
-                {
-                  for (int q = 0; q < nb; ++q)
-                    {
-                      double *Fq = d_fronts_ + nodes_[b.nodes[q]].off;
-                      if (cublasDtrsm(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                                      CUBLAS_DIAG_UNIT, b.nE, b.nK + 1, &one_, Fq, nF,
-                                      Fq + (int64_t)b.nE * nF, nF) != CUBLAS_STATUS_SUCCESS ||
-                          cublasDtrsm(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
-                                      CUBLAS_DIAG_NON_UNIT, b.nE, b.nK + 1, &one_, Fq, nF,
-                                      Fq + (int64_t)b.nE * nF, nF) != CUBLAS_STATUS_SUCCESS)
-                        return bad(err, "cublasDtrsm failed", DDHDG_SOLVER_ERROR);
-                    }
-                }
-              else if (cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                                          CUBLAS_DIAG_UNIT, b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF,
-                                          nb) != CUBLAS_STATUS_SUCCESS ||
-                       cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
-                                          CUBLAS_DIAG_NON_UNIT, b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF,
-                                          nb) != CUBLAS_STATUS_SUCCESS)
+              if (cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                                     CUBLAS_DIAG_UNIT, b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF,
+                                     nb) != CUBLAS_STATUS_SUCCESS ||
+                  cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                                     CUBLAS_DIAG_NON_UNIT, b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF,
+                                     nb) != CUBLAS_STATUS_SUCCESS)
                 return bad(err, "cublasDtrsmBatched failed", DDHDG_SOLVER_ERROR);
               if (b.nK > 0)
                 {
                   const double mone = -1., one = 1.;
-                  if (b.big)
-                    {
-                      for (int q = 0; q < nb; ++q)
-                        {
-                          double *Fq = d_fronts_ + nodes_[b.nodes[q]].off;
-                          if (cublasDgemm(blas_, CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE, &mone,
-                                          Fq + b.nE, nF, Fq + (int64_t)b.nE * nF, nF, &one,
-                                          Fq + (int64_t)b.nE * nF + b.nE, nF) != CUBLAS_STATUS_SUCCESS)
-                            return bad(err, "cublasDgemm failed", DDHDG_SOLVER_ERROR);
-                        }
-                    }
-                  else if (cublasDgemmBatched(blas_, CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE,
-                                              &mone, pKE, nF, pEK, nF, &one, pKK, nF,
-                                              nb) != CUBLAS_STATUS_SUCCESS)
+                  if (cublasDgemmBatched(blas_, CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE, &mone,
+                                         pKE, nF, pEK, nF, &one, pKK, nF, nb) != CUBLAS_STATUS_SUCCESS)
                     return bad(err, "cublasDgemmBatched failed", DDHDG_SOLVER_ERROR);
                 }
             }
@@ -595,6 +581,8 @@ namespace ddhdg
     }
 
   private:
+    static constexpr int NSide = 8; // side streams for the large fronts
+
     struct Node
     {
       int                  lo[3], hi[3];
@@ -614,6 +602,54 @@ namespace ddhdg
       bool             big     = false;
       int              maxc[2] = {0, 0}; // max child nK + 1 per extend-add pass
     };
+
+    // the large fronts of one batch (few, independent, each too small to
+    // fill the GPU alone): LU, row permutation, triangular solves and the
+    // Schur update per front, spread over the side streams
+    int
+    big_batch(const Batch &b, int info_base, cudaStream_t s, std::string &err)
+    {
+      const int nF = b.nE + b.nK;
+      const int nb = (int)b.nodes.size();
+      if (cudaEventRecord(ev_fork_, s) != cudaSuccess)
+        return bad(err, "cudaEventRecord failed", DDHDG_CUDA_ERROR);
+      const int used = std::min(nb, NSide);
+      for (int k = 0; k < used; ++k)
+        if (cudaStreamWaitEvent(side_[k], ev_fork_, 0) != cudaSuccess)
+          return bad(err, "cudaStreamWaitEvent failed", DDHDG_CUDA_ERROR);
+      const double one = 1., mone = -1.;
+      for (int q = 0; q < nb; ++q)
+        {
+          const int    k   = q % NSide;
+          cudaStream_t ss  = side_[k];
+          double      *Fq  = d_fronts_ + nodes_[b.nodes[q]].off;
+          int         *piv = d_piv_ + b.piv_off + (int64_t)q * b.nE;
+          int         *pm  = d_perm_ + b.piv_off + (int64_t)q * b.nE;
+          if (cusolverDnDgetrf(side_dn_[k], b.nE, b.nE, Fq, nF, d_work_ + (int64_t)k * work_per_,
+                               piv, d_info_ + info_base + q) != CUSOLVER_STATUS_SUCCESS)
+            return bad(err, "cusolverDnDgetrf failed", DDHDG_SOLVER_ERROR);
+          nd_pivperm_kernel<<<1, 32, 0, ss>>>(1, b.nE, piv, pm);
+          const dim3 g2(1, (b.nK + 1 + NDPermCols - 1) / NDPermCols);
+          nd_rowperm_kernel<<<g2, 256, b.nE * sizeof(double), ss>>>(b.nE, nF, d_sol_ + b.sol_off + q,
+                                                                    pm, d_fronts_);
+          double *B = Fq + (int64_t)b.nE * nF;
+          if (cublasDtrsm(side_blas_[k], CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                          CUBLAS_DIAG_UNIT, b.nE, b.nK + 1, &one, Fq, nF, B, nF) != CUBLAS_STATUS_SUCCESS ||
+              cublasDtrsm(side_blas_[k], CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                          CUBLAS_DIAG_NON_UNIT, b.nE, b.nK + 1, &one, Fq, nF, B, nF) != CUBLAS_STATUS_SUCCESS)
+            return bad(err, "cublasDtrsm failed", DDHDG_SOLVER_ERROR);
+          if (b.nK > 0 &&
+              cublasDgemm(side_blas_[k], CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE, &mone, Fq + b.nE,
+                          nF, B, nF, &one, B + b.nE, nF) != CUBLAS_STATUS_SUCCESS)
+            return bad(err, "cublasDgemm failed", DDHDG_SOLVER_ERROR);
+        }
+      for (int k = 0; k < used; ++k)
+        if (cudaEventRecord(ev_join_[k], side_[k]) != cudaSuccess ||
+            cudaStreamWaitEvent(s, ev_join_[k], 0) != cudaSuccess)
+          return bad(err, "stream join failed", DDHDG_CUDA_ERROR);
+      return DDHDG_OK;
+    }
+
 
     static int
     bad(std::string &err, const char *msg, int code = DDHDG_BAD_ARG)
@@ -778,6 +814,24 @@ namespace ddhdg
         cusolverDnDestroy(dn_);
       blas_  = nullptr;
       dn_    = nullptr;
+      for (int k = 0; k < NSide; ++k)
+        {
+          if (side_blas_[k])
+            cublasDestroy(side_blas_[k]);
+          if (side_dn_[k])
+            cusolverDnDestroy(side_dn_[k]);
+          if (ev_join_[k])
+            cudaEventDestroy(ev_join_[k]);
+          if (side_[k])
+            cudaStreamDestroy(side_[k]);
+          side_blas_[k] = nullptr;
+          side_dn_[k]   = nullptr;
+          ev_join_[k]   = nullptr;
+          side_[k]      = nullptr;
+        }
+      if (ev_fork_)
+        cudaEventDestroy(ev_fork_);
+      ev_fork_ = nullptr;
       built_ = false;
     }
 
@@ -807,5 +861,11 @@ namespace ddhdg
     unsigned long long *d_dmax_  = nullptr;
     cublasHandle_t      blas_    = nullptr;
     cusolverDnHandle_t  dn_      = nullptr;
+    cudaStream_t        side_[NSide]      = {};
+    cublasHandle_t      side_blas_[NSide] = {};
+    cusolverDnHandle_t  side_dn_[NSide]   = {};
+    cudaEvent_t         ev_join_[NSide]   = {};
+    cudaEvent_t         ev_fork_          = nullptr;
+    int64_t             work_per_         = 1;
   };
 } // namespace ddhdg
