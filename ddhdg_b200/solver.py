@@ -289,6 +289,87 @@ class NPSolver:
                    "reconstruct")
         return out.view(self.ncells, self.Nc_all)
 
+    # ------------------------------------------- global linear system
+    def assemble_system(self, thermo=False):
+        """assemble_system(false, thermo_eq) + copy_local_to_global
+        (include/assembling_methods.template.h:10-89, src/np_solver.cpp:
+        1293-1322) on the device: the Newton system of the trace at the
+        current state, kept as a CSR matrix (rows and columns in the
+        restricted trace order: face, enabled component, face node).
+        Dirichlet-constrained dofs are identity rows whose right-hand side is
+        the projected Dirichlet increment."""
+        torch = _torch()
+        s = self.sizes(thermo)
+        tt, rhs, flag, val = self.assemble_condense(thermo)
+        vals = torch.zeros(s.nnz, dtype=torch.float64, device=self.device)
+        grhs = torch.zeros(s.n_trace_dofs, dtype=torch.float64, device=self.device)
+        _lib.check(self.L.ddhdg_scatter(self._ctx, tt.data_ptr(), rhs.data_ptr(), flag.data_ptr(),
+                                        val.data_ptr(), vals.data_ptr(), grhs.data_ptr(), int(thermo),
+                                        self._sp()), "scatter")
+        self._system = dict(thermo=bool(thermo), blocks=(tt, rhs, flag, val), values=vals, rhs=grhs)
+        return self._system
+
+    def _need_system(self):
+        if getattr(self, "_system", None) is None:
+            self.assemble_system()
+        return self._system
+
+    def _component_dofs(self, thermo=False):
+        """restricted trace dof indices of every enabled component"""
+        comps = [0] if thermo else [c for c in range(3) if self.enabled[c]]
+        nc = len(comps)
+        idx = np.arange(self.nfaces * nc * self.nf).reshape(self.nfaces, nc, self.nf)
+        return {Component(c): idx[:, i, :].ravel() for i, c in enumerate(comps)}
+
+    def _csr_structure(self, thermo=False):
+        rp, ci = ctypes.c_void_p(), ctypes.c_void_p()
+        _lib.check(self.L.ddhdg_get_csr(self._ctx, int(thermo), ctypes.byref(rp), ctypes.byref(ci)), "get_csr")
+        s = self.sizes(thermo)
+        rowptr = np.empty(s.n_trace_dofs + 1, dtype=np.int32)
+        colind = np.empty(s.nnz, dtype=np.int32)
+        cudart = ctypes.CDLL("libcudart.so")
+        self.stream.synchronize()
+        for host, ptr in ((rowptr, rp), (colind, ci)):
+            if cudart.cudaMemcpy(host.ctypes.data_as(ctypes.c_void_p), ptr, ctypes.c_size_t(host.nbytes), 2):
+                raise RuntimeError("cudaMemcpy of the trace sparsity failed")
+        return rowptr, colind
+
+    def get_residual(self):
+        """pyddhdg NPSolver::get_residual (src/pyddhdg/pyddhdg.cpp:1601-1666):
+        the right-hand side of the assembled system, one array per enabled
+        component (dofs in the restricted trace order)."""
+        sysm = self._need_system()
+        b = sysm["rhs"].cpu().numpy()
+        return {c: b[d] for c, d in self._component_dofs(sysm["thermo"]).items()}
+
+    def get_jacobian(self):
+        """pyddhdg NPSolver::get_jacobian (src/pyddhdg/pyddhdg.cpp:1852-1935):
+        the assembled matrix split into blocks per pair of enabled
+        components, as scipy CSR matrices."""
+        import scipy.sparse as sp
+
+        sysm = self._need_system()
+        rowptr, colind = self._csr_structure(sysm["thermo"])
+        n = len(rowptr) - 1
+        A = sp.csr_matrix((sysm["values"].cpu().numpy(), colind, rowptr), shape=(n, n))
+        dofs = self._component_dofs(sysm["thermo"])
+        return {(c1, c2): A[d1][:, d2].tocsr() for c1, d1 in dofs.items() for c2, d2 in dofs.items()}
+
+    def get_linear_system_solution_vector(self):
+        """pyddhdg NPSolver::get_linear_system_solution_vector
+        (src/pyddhdg/pyddhdg.cpp:1670-1735): the solution of the assembled
+        system (nested-dissection solve on the device), per enabled
+        component."""
+        torch = _torch()
+        sysm = self._need_system()
+        tt, rhs, flag, val = sysm["blocks"]
+        x = torch.empty(sysm["rhs"].numel(), dtype=torch.float64, device=self.device)
+        _lib.check(self.L.ddhdg_solve_condensed(self._ctx, tt.data_ptr(), rhs.data_ptr(), flag.data_ptr(),
+                                                val.data_ptr(), x.data_ptr(), int(sysm["thermo"]),
+                                                self._sp()), "solve_condensed")
+        xs = x.cpu().numpy()
+        return {c: xs[d] for c, d in self._component_dofs(sysm["thermo"]).items()}
+
     def private_run(self, abs_tol, rel_tol, max_it, thermo=False, alpha=None):
         alpha = self.parameters.nonlinear_parameters.alpha if alpha is None else alpha
         it = ctypes.c_int()
