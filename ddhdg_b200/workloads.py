@@ -78,3 +78,23 @@ def set_bias(problem, bias):
     bh.replace_boundary_condition(1, BCT.DIRICHLET, Component.V, Vp)
     bh.replace_boundary_condition(1, BCT.DIRICHLET, Component.n, density(Component.n, bias, Vp))
     bh.replace_boundary_condition(1, BCT.DIRICHLET, Component.p, density(Component.p, bias, Vp))
+
+
+def bias_sweep(solver, problem, biases, absolute_tol=None, relative_tol=None,
+               max_number_of_iterations=None, callback=None):
+    """Forward bias sweep with warm starts (the second diode configuration:
+    0 to 0.8 V in 0.05 V steps): for every bias the contact conditions are
+    replaced on the device (replace_boundary_condition,
+    src/np_solver.cpp:2160-2233, without rebuilding the sparsity) and Newton
+    starts from the previous bias point's solution.  Returns
+    [(bias, NonlinearIterationResults)]; `callback(bias, solver, result)` is
+    called after every point."""
+    out = []
+    for v in biases:
+        set_bias(problem, float(v))
+        solver.update_boundary_tables()
+        res = solver.run(absolute_tol, relative_tol, max_number_of_iterations)
+        out.append((float(v), res))
+        if callback is not None:
+            callback(float(v), solver, res)
+    return out
