@@ -221,6 +221,46 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_bias_sweep(args):
+    """The second diode configuration end to end: equilibrium, then a forward
+    bias sweep 0.0..0.8 V in 0.05 V steps, each point warm-started, every
+    Newton step on the device (assembly + condensation, nested-dissection
+    trace solve, reconstruction).  Consistent Jacobian (the reference's
+    diverges on this diode)."""
+    import torch
+
+    from ddhdg_b200 import workloads as cases
+    from ddhdg_b200.solver import NPSolver
+
+    m_side = args.cells_per_side
+    pb, prm, adim = cases.diode(dim=WORKLOAD["dim"], m=m_side, k=WORKLOAD["k"], length=m_side / WORKLOAD["m"])
+    prm.consistent_drift_jacobian = True
+    prm.consistent_recombination_jacobian = True
+    g = NPSolver(pb, prm, adim)
+    t0 = time.perf_counter()
+    req = g.compute_thermodynamic_equilibrium()
+    torch.cuda.synchronize()
+    t_eq = time.perf_counter() - t0
+    biases = [0.05 * i for i in range(17)]
+    steps, points = 0, []
+    t0 = time.perf_counter()
+
+    def keep(v, s, r):
+        points.append({"bias": round(v, 3), "iterations": r.iterations, "converged": bool(r.converged)})
+
+    cases.bias_sweep(g, pb, biases, 1e-10, 1e-10, 50, callback=keep)
+    torch.cuda.synchronize()
+    t_sweep = time.perf_counter() - t0
+    steps = sum(p["iterations"] for p in points)
+    line = {"metric": "bias sweep wall time (17 points, warm-started Newton)", "value": t_sweep, "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"2D p-n diode {m_side}x{m_side} quads, HDG degree 2, FP64, 0..0.8 V",
+                       "trace_dofs": int(g.sizes().n_trace_dofs), "cells": g.ncells},
+            "equilibrium_s": t_eq, "equilibrium_iterations": req.iterations,
+            "newton_steps": steps, "ms_per_newton_step": 1e3 * t_sweep / max(steps, 1), "points": points}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -228,11 +268,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bias-sweep", action="store_true",
+                    help="time the warm-started 0..0.8 V sweep (17 points) instead of the step")
     ap.add_argument("--cells-per-side", type=int, default=WORKLOAD["m"],
                     help="smaller meshes of the same diode for profiling runs")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.bias_sweep:
+        return run_bias_sweep(args)
 
     import torch
     import torch.distributed as dist
