@@ -24,6 +24,27 @@ namespace ddhdg
 {
   constexpr int Condense3MaxWPB = 8; // warps (cells) per CTA at most
 
+  // D += A B for one 8x8x4 FP64 tile on the tensor path (mma.sync m8n8k4):
+  // lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}]
+  __device__ __forceinline__ void
+  dmma8x8x4(double &d0, double &d1, double a, double b)
+  {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+  }
+
+  // row stride of the staged S^-1 (>= its padded width, = 4 mod 16 doubles:
+  // the A-fragment loads of a half warp hit 16 different 8-byte banks)
+  __host__ __device__ constexpr int
+  sinv_stride(int nsmax)
+  {
+    int kp = (nsmax + 3) / 4 * 4;
+    while (kp % 16 != 4)
+      ++kp;
+    return kp;
+  }
+
   // Constant tables read at lane-uniform addresses in fully unrolled loops.
   // They travel as a kernel parameter (constant bank), so that the FMAs take
   // them as constant operands; at most 14.4 KB (3D, degree 1).
@@ -98,6 +119,12 @@ namespace ddhdg
     o.rZ  = take(Nt);
     o.H   = take(3 * Fq);
     p     = p > dead_end ? p : dead_end;
+    {
+      // staged S^-1 of the tensor-path Y = S^-1 R ([rows padded to 8][stride])
+      const int sv = (3 * nb + 7) / 8 * 8 * sinv_stride(3 * nb);
+      p            = p > sv ? p : sv;
+      p            = (p + 1) & ~1;
+    }
     o.tcS  = take(3 * Fq);
     o.tcW  = take(9 * Fq);
     o.ttc  = take(3 * Fq);
@@ -812,42 +839,58 @@ namespace ddhdg
             srow[k] *= dsc[k];
         }
 
-        // ---------- Y = S^-1 R, row mypos per lane, written back over R
-        for (int c0_ = 0; c0_ < ncol; c0_ += 16)
-          {
-            double acc[16];
+        // ---------- Y = S^-1 R on the FP64 tensor path, written back over R
+        {
+          constexpr int MP = (NSMAX + 7) / 8 * 8;
+          constexpr int KP = (NSMAX + 3) / 4 * 4;
+          constexpr int KS = sinv_stride(NSMAX);
+          double       *Sv = coef; // the coefficient block is dead here
+          for (int idx = lane; idx < MP * KS; idx += 32)
+            Sv[idx] = 0.;
+          __syncwarp();
+          if (act)
+            {
 #pragma unroll
-            for (int u = 0; u < 16; ++u)
-              acc[u] = 0.;
-            if (act)
-              {
+              for (int k = 0; k < NSMAX; ++k)
+                Sv[mypos * KS + k] = srow[k];
+            }
+          __syncwarp();
+          const int g = lane >> 2, tq = lane & 3;
+          for (int n0 = 0; n0 < ncol; n0 += 8)
+            {
+              const int col = n0 + g;
+              double    bf[KP / 4];
 #pragma unroll
-                for (int k = 0; k < NSMAX; ++k)
-                  if (k < Ns)
+              for (int ks = 0; ks < KP / 4; ++ks)
+                {
+                  const int kk = ks * 4 + tq;
+                  bf[ks]       = (kk < Ns && col < ncol) ? R[piv3[warp][kk] * ldr + col] : 0.;
+                }
+              double acc[MP / 8][2];
+#pragma unroll
+              for (int mt = 0; mt < MP / 8; ++mt)
+                {
+                  acc[mt][0] = acc[mt][1] = 0.;
+#pragma unroll
+                  for (int ks = 0; ks < KP / 4; ++ks)
+                    dmma8x8x4(acc[mt][0], acc[mt][1], Sv[(mt * 8 + g) * KS + ks * 4 + tq], bf[ks]);
+                }
+              __syncwarp(); // every lane has read this block of R columns
+#pragma unroll
+              for (int mt = 0; mt < MP / 8; ++mt)
+                {
+                  const int row = mt * 8 + g;
+#pragma unroll
+                  for (int e = 0; e < 2; ++e)
                     {
-                      const double   sk = srow[k];
-                      const double2 *rk =
-                        reinterpret_cast<const double2 *>(R + piv3[warp][k] * ldr + c0_);
-#pragma unroll
-                      for (int v = 0; v < 8; ++v)
-                        if (c0_ + 2 * v < ncol)
-                          {
-                            const double2 x = rk[v];
-                            acc[2 * v] += sk * x.x;
-                            acc[2 * v + 1] += sk * x.y;
-                          }
+                      const int c = n0 + 2 * tq + e;
+                      if (row < Ns && c < ncol)
+                        R[row * ldr + c] = acc[mt][e];
                     }
-              }
-            __syncwarp();
-            if (act)
-              {
-#pragma unroll
-                for (int u = 0; u < 16; ++u)
-                  if (c0_ + u < ncol)
-                    R[mypos * ldr + c0_ + u] = acc[u];
-              }
-            __syncwarp();
-          }
+                }
+              __syncwarp();
+            }
+        }
         double *const Y = R;
 
         // ------------------------ keep Y for the reconstruction [col][row]
@@ -961,81 +1004,54 @@ namespace ddhdg
             P.dval[cell * Nt + i]  = gv[i];
           }
 
-        // ------ tt = T Y_t + tc_W Q_t + face block, 4 x 8 lane grid of tiles
+        // ---- tt = T Y_comb + tc_W Q_t + face block, FP64 tensor-path tiles
         {
-          constexpr int NTM = F * 3 * nf;
-          constexpr int TC  = (NTM + 7) / 8;
-          constexpr int TR0 = (NTM + 3) / 4;
-          constexpr int TR  = TR0 < 9 ? TR0 : 9;
-          const int     lr = lane >> 3, lc = lane & 7;
+          constexpr int KP     = (NSMAX + 3) / 4 * 4;
+          const int     g      = lane >> 2, tq = lane & 3;
           double       *tt_out = P.tt + cell * (int64_t)Nt * Nt;
-          int           ft_[TC], ct_[TC], mt_[TC];
-          bool          cok[TC];
-#pragma unroll
-          for (int b = 0; b < TC; ++b)
+          for (int m0 = 0; m0 < Nt; m0 += 8)
             {
-              const int t = lc + 8 * b;
-              ft_[b]      = t / (ncomp * nf);
-              ct_[b]      = (t / nf) % ncomp;
-              mt_[b]      = t % nf;
-              cok[b]      = t < Nt && dfl[t < Nt ? t : 0] == 0.;
-            }
-          for (int r0_ = 0; r0_ < Nt; r0_ += 4 * TR)
-            {
-              double acc[TR][TC];
+              const int i = m0 + g; // output row of this lane
+              double    af[KP / 4];
 #pragma unroll
-              for (int a2 = 0; a2 < TR; ++a2)
-#pragma unroll
-                for (int b = 0; b < TC; ++b)
-                  acc[a2][b] = 0.;
-#pragma unroll 1
-              for (int j = 0; j < Ns; ++j)
+              for (int ks = 0; ks < KP / 4; ++ks)
                 {
-                  double ta[TR], yb[TC];
-#pragma unroll
-                  for (int a2 = 0; a2 < TR; ++a2)
-                    {
-                      const int i = r0_ + lr + 4 * a2;
-                      ta[a2]      = (i < Nt) ? Trs[j * Nt + i] : 0.;
-                    }
-#pragma unroll
-                  for (int b = 0; b < TC; ++b)
-                    {
-                      const int t = lc + 8 * b;
-                      yb[b]       = (t < Nt) ? Y[j * ldr + colC + t] : 0.;
-                    }
-#pragma unroll
-                  for (int a2 = 0; a2 < TR; ++a2)
-#pragma unroll
-                    for (int b = 0; b < TC; ++b)
-                      acc[a2][b] += ta[a2] * yb[b];
+                  const int j = ks * 4 + tq;
+                  af[ks]      = (i < Nt && j < Ns) ? Trs[j * Nt + i] : 0.;
                 }
-#pragma unroll
-              for (int a2 = 0; a2 < TR; ++a2)
+              const int  ii  = i < Nt ? i : 0;
+              const int  fi  = ii / (ncomp * nf), ci2 = (ii / nf) % ncomp;
+              const bool rok = i < Nt && dfl[ii] == 0.;
+              for (int n0 = 0; n0 < Nt; n0 += 8)
                 {
-                  const int i = r0_ + lr + 4 * a2;
-                  if (i >= Nt)
-                    continue;
-                  const int  fi = i / (ncomp * nf), ci2 = (i / nf) % ncomp;
-                  const bool rok = dfl[i] == 0.;
+                  double    d[2] = {0., 0.};
+                  const int tb   = n0 + g; // B-fragment column
 #pragma unroll
-                  for (int b = 0; b < TC; ++b)
+                  for (int ks = 0; ks < KP / 4; ++ks)
                     {
-                      const int t = lc + 8 * b;
-                      if (t >= Nt)
+                      const int    j  = ks * 4 + tq;
+                      const double bv = (j < Ns && tb < Nt) ? Y[j * ldr + colC + tb] : 0.;
+                      dmma8x8x4(d[0], d[1], af[ks], bv);
+                    }
+#pragma unroll
+                  for (int e = 0; e < 2; ++e)
+                    {
+                      const int t = n0 + 2 * tq + e;
+                      if (i >= Nt || t >= Nt)
                         continue;
                       double o = 0.;
-                      if (rok && cok[b])
+                      if (rok && dfl[t] == 0.)
                         {
-                          const int tq = ft_[b] * nf + mt_[b];
-                          double    z  = acc[a2][b];
+                          const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
+                          const int tqq = ft * nf + mt;
+                          double    z   = d[e];
 #pragma unroll
                           for (int qf = 0; qf < nqf; ++qf)
-                            z += rA[(i * 3 + ct_[b]) * nqf + qf] * RQr[(fi * nqf + qf) * Ft + tq];
-                          if (ft_[b] == fi && ct_[b] == ci2)
+                            z += rA[(i * 3 + ct) * nqf + qf] * RQr[(fi * nqf + qf) * Ft + tqq];
+                          if (ft == fi && ct == ci2)
 #pragma unroll
                             for (int qf = 0; qf < nqf; ++qf)
-                              z += rD[i * nqf + qf] * xi[qf * nf + mt_[b]];
+                              z += rD[i * nqf + qf] * xi[qf * nf + mt];
                           o = z;
                         }
                       tt_out[(int64_t)i * Nt + t] = o;
