@@ -1006,57 +1006,75 @@ namespace ddhdg
 
         // ---- tt = T Y_comb + tc_W Q_t + face block, FP64 tensor-path tiles
         {
+          constexpr int NTM    = F * 3 * nf;
+          constexpr int NNT    = (NTM + 7) / 8; // column tiles (all enabled components)
           constexpr int KP     = (NSMAX + 3) / 4 * 4;
           const int     g      = lane >> 2, tq = lane & 3;
           double       *tt_out = P.tt + cell * (int64_t)Nt * Nt;
+          // this lane's output columns t = 8 nt + 2 tq + e, decoded once:
+          // face | component << 4 | node << 8 | (usable column) << 15
+          int cm[NNT][2];
+#pragma unroll
+          for (int nt = 0; nt < NNT; ++nt)
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+              {
+                const int t  = nt * 8 + 2 * tq + e;
+                const int tt = t < Nt ? t : 0;
+                cm[nt][e]    = (tt / (ncomp * nf)) | (((tt / nf) % ncomp) << 4) | ((tt % nf) << 8) |
+                            ((t < Nt && dfl[tt] == 0.) ? (1 << 15) : 0);
+              }
           for (int m0 = 0; m0 < Nt; m0 += 8)
             {
               const int i = m0 + g; // output row of this lane
-              double    af[KP / 4];
+              double    d[NNT][2];
+#pragma unroll
+              for (int nt = 0; nt < NNT; ++nt)
+                d[nt][0] = d[nt][1] = 0.;
 #pragma unroll
               for (int ks = 0; ks < KP / 4; ++ks)
                 {
-                  const int j = ks * 4 + tq;
-                  af[ks]      = (i < Nt && j < Ns) ? Trs[j * Nt + i] : 0.;
-                }
-              const int  ii  = i < Nt ? i : 0;
-              const int  fi  = ii / (ncomp * nf), ci2 = (ii / nf) % ncomp;
-              const bool rok = i < Nt && dfl[ii] == 0.;
-              for (int n0 = 0; n0 < Nt; n0 += 8)
-                {
-                  double    d[2] = {0., 0.};
-                  const int tb   = n0 + g; // B-fragment column
+                  const int    j  = ks * 4 + tq;
+                  const double av = (i < Nt && j < Ns) ? Trs[j * Nt + i] : 0.;
 #pragma unroll
-                  for (int ks = 0; ks < KP / 4; ++ks)
+                  for (int nt = 0; nt < NNT; ++nt)
                     {
-                      const int    j  = ks * 4 + tq;
+                      const int    tb = nt * 8 + g; // B-fragment column
                       const double bv = (j < Ns && tb < Nt) ? Y[j * ldr + colC + tb] : 0.;
-                      dmma8x8x4(d[0], d[1], af[ks], bv);
+                      dmma8x8x4(d[nt][0], d[nt][1], av, bv);
                     }
+                }
+              if (i >= Nt)
+                continue;
+              const int  fi  = i / (ncomp * nf), ci2 = (i / nf) % ncomp;
+              const bool rok = dfl[i] == 0.;
+              const double *rAi = rA + i * 3 * nqf, *rDi = rD + i * nqf;
 #pragma unroll
-                  for (int e = 0; e < 2; ++e)
-                    {
-                      const int t = n0 + 2 * tq + e;
-                      if (i >= Nt || t >= Nt)
-                        continue;
-                      double o = 0.;
-                      if (rok && dfl[t] == 0.)
-                        {
-                          const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
-                          const int tqq = ft * nf + mt;
-                          double    z   = d[e];
+              for (int nt = 0; nt < NNT; ++nt)
+#pragma unroll
+                for (int e = 0; e < 2; ++e)
+                  {
+                    const int t = nt * 8 + 2 * tq + e;
+                    if (t >= Nt)
+                      continue;
+                    const int c  = cm[nt][e];
+                    double    o  = 0.;
+                    if (rok && (c >> 15))
+                      {
+                        const int ft = c & 15, ct = (c >> 4) & 15, mt = (c >> 8) & 127;
+                        const int tqq = ft * nf + mt;
+                        double    z   = d[nt][e];
+#pragma unroll
+                        for (int qf = 0; qf < nqf; ++qf)
+                          z += rAi[ct * nqf + qf] * RQr[(fi * nqf + qf) * Ft + tqq];
+                        if (ft == fi && ct == ci2)
 #pragma unroll
                           for (int qf = 0; qf < nqf; ++qf)
-                            z += rA[(i * 3 + ct) * nqf + qf] * RQr[(fi * nqf + qf) * Ft + tqq];
-                          if (ft == fi && ct == ci2)
-#pragma unroll
-                            for (int qf = 0; qf < nqf; ++qf)
-                              z += rD[i * nqf + qf] * xi[qf * nf + mt];
-                          o = z;
-                        }
-                      tt_out[(int64_t)i * Nt + t] = o;
-                    }
-                }
+                            z += rDi[qf] * xi[qf * nf + mt];
+                        o = z;
+                      }
+                    tt_out[(int64_t)i * Nt + t] = o;
+                  }
             }
         }
         __syncwarp();
