@@ -98,8 +98,8 @@ def fp64_peak_tflops(dev):
 
 # DRAM bytes (read + write) of one condense launch per cell, from the ncu
 # capture summarised in profiles/condense3_2d_k2.md (16 384 cells: 14.8 MB
-# read + 260.1 MB written), scaled to a launch by the cells it processes
-TRAFFIC_BYTES_PER_CELL = 16779
+# read + 260.6 MB written), scaled to a launch by the cells it processes
+TRAFFIC_BYTES_PER_CELL = 16806
 
 
 def bytes_per_cell(dim, k, ncomp=3):
