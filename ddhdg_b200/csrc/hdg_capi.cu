@@ -1240,7 +1240,7 @@ ddhdg_reconstruct(ddhdg_ctx *c, const double *cell_state, const double *trace_st
   P.trace_state = trace_state;
   P.ycache      = m.ycache.p;
   const int    Ns  = m.ncomp * c->nb;
-  const int    wsz = (Ns + 2 * c->F * 3 * c->nf + c->nb + 1) & ~1;
+  const int    wsz = (Ns + 2 * c->F * 3 * c->nf + c->nb + m.Nt + 1) & ~1;
   const int    wpb = 8;
   const size_t nPQ = (size_t)(c->to.minv - c->to.P);
   const size_t smem =

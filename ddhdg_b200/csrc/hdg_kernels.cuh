@@ -111,12 +111,13 @@ namespace ddhdg
     __syncthreads();
     const double *Pm  = smem;
     const double *Qm  = smem + (P.to.Q - P.to.P);
-    const int     wsz = Ns + 2 * F * 3 * nf + nb;
+    const int     wsz = Ns + 2 * F * 3 * nf + nb + Nt;
     double *ws   = smem + ((nPQ + 1) & ~1) + warp * ((wsz + 1) & ~1);
     double *du   = ws;
     double *dl   = ws + Ns;          // [F][3][nf] trace update
     double *lnew = dl + F * 3 * nf;  // [F][3][nf] lam0 + dlam
     double *unew = lnew + F * 3 * nf;
+    double *dlr  = unew + nb;        // [Nt] trace update, restricted order
 
     for (int64_t cell = (int64_t)blockIdx.x * P.wpb + warp; cell < P.ncells;
          cell += (int64_t)gridDim.x * P.wpb)
@@ -130,18 +131,30 @@ namespace ddhdg
             lnew[i]          = P.trace_state[Fi * 3 * nf + (i % (3 * nf))] + d;
           }
         __syncwarp();
+        for (int t = lane; t < Nt; t += 32)
+          {
+            const int f  = t / (ncomp * nf);
+            const int ce = (t / nf) % ncomp;
+            const int b  = ce == 0 ? P.comps[0] : (ce == 1 ? P.comps[1] : P.comps[2]);
+            dlr[t]       = dl[(f * 3 + b) * nf + t % nf];
+          }
+        __syncwarp();
         const double *Y = P.ycache + cell * (int64_t)Ns * P.ycols;
         for (int i = lane; i < Ns; i += 32)
           {
-            double v = Y[i];
-            for (int t = 0; t < Nt; ++t)
+            const double *Yi = Y + Ns + i;
+            double        v0 = Y[i], v1 = 0., v2 = 0., v3 = 0.;
+            int           t  = 0;
+            for (; t + 4 <= Nt; t += 4)
               {
-                const int f  = t / (ncomp * nf);
-                const int ce = (t / nf) % ncomp;
-                const int m  = t % nf;
-                v -= Y[(1 + t) * Ns + i] * dl[(f * 3 + P.comps[ce]) * nf + m];
+                v0 -= Yi[(t + 0) * Ns] * dlr[t + 0];
+                v1 -= Yi[(t + 1) * Ns] * dlr[t + 1];
+                v2 -= Yi[(t + 2) * Ns] * dlr[t + 2];
+                v3 -= Yi[(t + 3) * Ns] * dlr[t + 3];
               }
-            du[i] = v;
+            for (; t < Nt; ++t)
+              v0 -= Yi[t * Ns] * dlr[t];
+            du[i] = (v0 + v1) + (v2 + v3);
           }
         __syncwarp();
         const double *cs  = P.cell_state + cell * NCA;
