@@ -221,6 +221,158 @@ namespace ddhdg
       }
   }
 
+  // Small fronts (nE <= NDSmallE): the whole elimination of a front in one
+  // CTA.  F_EE and [F_EK | r_E] are staged in shared memory; LU with partial
+  // pivoting (row swaps in shared memory), back substitution to
+  // W = F_EE^-1 [F_EK | r_E] (written back to the front for the downward
+  // pass), then F_KK -= F_KE W in global memory with 4 x 4 register tiles
+  // (F_KE read from the front, coalesced over rows).  info[front] = first
+  // zero pivot (1-based) or 0.
+  constexpr int NDSmallE = 36;
+
+  __global__ void
+  nd_small_front_kernel(int nE, int nK, const NDSol *nodes, int *info, double *fronts)
+  {
+    extern __shared__ double sm[];
+    __shared__ int     piv_s, sing_s;
+    const int          nF = nE + nK, nc = nK + 1;
+    double            *A  = sm;              // [nE][nE]  column-major
+    double            *B  = A + nE * nE;     // [nE][nc]  column-major
+    double            *Fv = fronts + nodes[blockIdx.x].off;
+    const int          tid = threadIdx.x, T = blockDim.x;
+    for (int idx = tid; idx < nE * nE; idx += T)
+      A[idx] = Fv[(int64_t)(idx / nE) * nF + idx % nE];
+    for (int idx = tid; idx < nE * nc; idx += T)
+      B[idx] = Fv[(int64_t)(nE + idx / nE) * nF + idx % nE];
+    if (tid == 0)
+      sing_s = 0;
+    __syncthreads();
+    for (int j = 0; j < nE; ++j)
+      {
+        if (tid < 32)
+          {
+            double best = -1.;
+            int    bi   = nE;
+            for (int i = j + tid; i < nE; i += 32)
+              {
+                const double v = fabs(A[i + j * nE]);
+                if (v > best)
+                  {
+                    best = v;
+                    bi   = i;
+                  }
+              }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+              {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int    oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi))
+                  {
+                    best = ob;
+                    bi   = oi;
+                  }
+              }
+            if (tid == 0)
+              {
+                piv_s = (bi < nE) ? bi : j;
+                if (!(best > 0.) || !isfinite(best))
+                  if (sing_s == 0)
+                    sing_s = j + 1;
+              }
+          }
+        __syncthreads();
+        const int p = piv_s;
+        if (p != j)
+          for (int c = tid; c < nE + nc; c += T)
+            {
+              double *X = (c < nE) ? A + c * nE : B + (c - nE) * nE;
+              const double t = X[j];
+              X[j]           = X[p];
+              X[p]           = t;
+            }
+        __syncthreads();
+        const double d  = A[j + j * nE];
+        const double hr = (d != 0.) ? 1. / d : 0.;
+        for (int i = j + 1 + tid; i < nE; i += T)
+          A[i + j * nE] *= hr;
+        __syncthreads();
+        const int nr = nE - j - 1;
+        if (nr > 0)
+          for (int idx = tid; idx < nr * (nr + nc); idx += T)
+            {
+              const int i = j + 1 + idx % nr, c = idx / nr;
+              double   *X = (c < nr) ? A + (j + 1 + c) * nE : B + (c - nr) * nE;
+              X[i] -= A[i + j * nE] * X[j];
+            }
+        __syncthreads();
+      }
+    // back substitution with U
+    for (int j = nE - 1; j >= 0; --j)
+      {
+        const double d  = A[j + j * nE];
+        const double hr = (d != 0.) ? 1. / d : 0.;
+        for (int c = tid; c < nc; c += T)
+          B[j + c * nE] *= hr;
+        __syncthreads();
+        if (j > 0)
+          for (int idx = tid; idx < j * nc; idx += T)
+            {
+              const int i = idx % j, c = idx / j;
+              B[i + c * nE] -= A[i + j * nE] * B[j + c * nE];
+            }
+        __syncthreads();
+      }
+    for (int idx = tid; idx < nE * nc; idx += T)
+      Fv[(int64_t)(nE + idx / nE) * nF + idx % nE] = B[idx];
+    // Schur update of the kept block and the kept rhs: thread tile of rows
+    // i0 + r nrt (r < 4, consecutive threads take consecutive rows) and
+    // columns c0 .. c0 + 3
+    {
+      constexpr int RT = 4, CT = 4;
+      const int     nrt = (nK + RT - 1) / RT, nct = (nc + CT - 1) / CT;
+      for (int tile = tid; tile < nrt * nct; tile += T)
+        {
+          const int i0 = tile % nrt, c0 = (tile / nrt) * CT;
+          double    acc[RT][CT];
+#pragma unroll
+          for (int r = 0; r < RT; ++r)
+#pragma unroll
+            for (int q = 0; q < CT; ++q)
+              acc[r][q] = 0.;
+          for (int k = 0; k < nE; ++k)
+            {
+              double cv[RT], bv[CT];
+#pragma unroll
+              for (int r = 0; r < RT; ++r)
+                {
+                  const int i = i0 + r * nrt;
+                  cv[r]       = (i < nK) ? Fv[(int64_t)k * nF + nE + i] : 0.;
+                }
+#pragma unroll
+              for (int q = 0; q < CT; ++q)
+                bv[q] = (c0 + q < nc) ? B[k + (c0 + q) * nE] : 0.;
+#pragma unroll
+              for (int r = 0; r < RT; ++r)
+#pragma unroll
+                for (int q = 0; q < CT; ++q)
+                  acc[r][q] += cv[r] * bv[q];
+            }
+#pragma unroll
+          for (int r = 0; r < RT; ++r)
+#pragma unroll
+            for (int q = 0; q < CT; ++q)
+              {
+                const int i = i0 + r * nrt, c = c0 + q;
+                if (i < nK && c < nc)
+                  Fv[(int64_t)(nE + c) * nF + nE + i] -= acc[r][q];
+              }
+        }
+    }
+    if (tid == 0)
+      info[blockIdx.x] = sing_s;
+  }
+
   // -------------------------------------------------------------- host side
   class NDSolver
   {
@@ -391,6 +543,7 @@ namespace ddhdg
                                           : o + (int64_t)b.nE * nF + b.nE);
               }
           b.big   = b.nE >= 384 && b.nodes.size() <= 32;
+          b.small = !b.big && b.nE > 0 && b.nE <= NDSmallE && small_smem(b.nE, b.nK) <= 200 * 1024;
           max_nK_ = std::max(max_nK_, b.nK);
         }
       return DDHDG_OK;
@@ -456,6 +609,14 @@ namespace ddhdg
           cublasSetStream(side_blas_[k], side_[k]);
           cusolverDnSetStream(side_dn_[k], side_[k]);
         }
+      size_t max_small = 0;
+      for (auto &b : batches_)
+        if (b.small)
+          max_small = std::max(max_small, small_smem(b.nE, b.nK));
+      if (max_small > 48 * 1024)
+        if (cudaFuncSetAttribute(nd_small_front_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)max_small) != cudaSuccess)
+          return bad(err, "front too large for the fused small-front kernel", DDHDG_SOLVER_ERROR);
       int max_nE = 0;
       for (auto &b : batches_)
         max_nE = std::max(max_nE, b.nE);
@@ -518,6 +679,13 @@ namespace ddhdg
               double **pEE = d_ptr_ + b.ptr_off, **pEK = pEE + nb, **pKE = pEK + nb, **pKK = pKE + nb;
               int     *piv = d_piv_ + b.piv_off;
               int     *inf = d_info_ + info_base;
+              if (b.small)
+                {
+                  nd_small_front_kernel<<<nb, 256, small_smem(b.nE, b.nK), s>>>(
+                    b.nE, b.nK, d_sol_ + b.sol_off, d_info_ + info_base, d_fronts_);
+                  info_base += nb;
+                  continue;
+                }
               if (b.big)
                 {
                   int r;
@@ -601,7 +769,14 @@ namespace ddhdg
       int64_t          front_off = 0, front_end = 0, piv_off = 0, asm_off = 0, sol_off = 0, ptr_off = 0;
       bool             big     = false;
       int              maxc[2] = {0, 0}; // max child nK + 1 per extend-add pass
+      bool             small   = false;  // fused one-CTA elimination
     };
+
+    static size_t
+    small_smem(int nE, int nK)
+    {
+      return ((size_t)nE * nE + (size_t)nE * (nK + 1)) * sizeof(double);
+    }
 
     // the large fronts of one batch (few, independent, each too small to
     // fill the GPU alone): LU, row permutation, triangular solves and the
