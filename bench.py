@@ -297,6 +297,7 @@ def main():
     _b.build()
     from ddhdg_b200.solver import NPSolver
     from ddhdg_b200 import _lib
+    from ddhdg_b200 import replicas
     from ddhdg_b200 import workloads as cases
 
     m_side = args.cells_per_side
@@ -337,8 +338,7 @@ def main():
     # ---- device-resident timing (inputs in HBM; per-step traffic > L2)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps + 2)]
     sampler = ClockSampler(local)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     sampler.start()
     time.sleep(0.3)
@@ -355,12 +355,9 @@ def main():
     total_ms = ev[0].elapsed_time(ev[-1])
     cond_ms = [ev[1 + 3 * i].elapsed_time(ev[2 + 3 * i]) for i in range(args.steps)]
     rec_ms = [ev[2 + 3 * i].elapsed_time(ev[3 + 3 * i]) for i in range(args.steps)]
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = replicas.max_over_ranks(total_ms, dev)
     ms_per_step = total_ms / args.steps
-    value = world * nc / (ms_per_step * 1e-3)
+    value = replicas.job_throughput(nc, ms_per_step)
 
     # ---- end to end through the C ABI with host buffers
     pin_cell = torch.empty(nc * g.Nc_all, dtype=torch.float64).pin_memory()
@@ -385,18 +382,14 @@ def main():
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     e0.record(stream)
     for _ in range(args.steps):
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    t2 = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t2.item()) / args.steps
-    e2e_value = world * nc / (e2e_ms * 1e-3)
+    e2e_ms = replicas.max_over_ranks(e0.elapsed_time(e1), dev) / args.steps
+    e2e_value = replicas.job_throughput(nc, e2e_ms)
 
     # ---- one whole Newton step (BASELINE's second metric): assembly +
     # condensation, nested-dissection trace solve, reconstruction, norms and
@@ -410,13 +403,15 @@ def main():
     torch.cuda.synchronize()
     newton_steps = 3
     gn.set_state(g.get_cell_state(), g.get_trace_state())
+    replicas.barrier()
     en0, en1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     en0.record(gn.stream)
     gn.private_run(0.0, 0.0, newton_steps)
     en1.record(gn.stream)
     torch.cuda.synchronize()
     nt = gn.last_timings()
-    newton = {"ms": en0.elapsed_time(en1) / newton_steps, "steps": newton_steps,
+    newton = {"ms": replicas.max_over_ranks(en0.elapsed_time(en1), dev) / newton_steps,
+              "steps": newton_steps,
               "stages_ms": {"assemble_condense": nt["condense_ms"] / nt["steps"],
                             "trace_solve": nt["solve_ms"] / nt["steps"],
                             "reconstruct": nt["reconstruct_ms"] / nt["steps"]},
