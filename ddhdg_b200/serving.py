@@ -1,0 +1,214 @@
+"""Serving: a request loop for diode solves of different sizes.
+
+Requests (a diode's dimension, mesh, degree and bias) arrive over time.  The
+server admits a request as soon as an in-flight slot and enough free device
+memory are available.  Every admitted request runs in its own host worker
+thread, with its own context and its own CUDA stream, so that the device work
+of the requests in flight overlaps; their Newton state stays on the device
+for the whole solve.  The C calls release the GIL, so the workers' host sides
+interleave as well.  Results do not depend on what else runs: every kernel is
+deterministic (no atomics with more than two contributions, no
+order-dependent reductions), so a request's fields are the same alone and in
+the mix.
+
+A solve is: thermodynamic equilibrium (charge-neutral first guess, V-only
+Newton, density projection), then, for a nonzero bias, the contact
+conditions for that bias and the Newton solve warm-started from equilibrium.
+The consistent Jacobian is used (the reference's diverges on these diodes).
+"""
+
+from __future__ import annotations
+
+import math
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    rid: int
+    dim: int
+    m: int          # cells per side
+    k: int          # degree
+    bias: float     # volts on the p contact
+    arrival: float  # seconds after the start of the run
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    start: float
+    finish: float
+    iterations: int
+    converged: bool
+    cells: int
+    state: tuple = field(default=None, repr=False)  # (cell, trace) on the host, if kept
+
+    @property
+    def latency(self):
+        return self.finish - self.arrival
+
+
+def memory_estimate(dim: int, m: int, k: int) -> int:
+    """Device bytes of one solve: states, condensed blocks, the Y cache and
+    the fronts of the nested-dissection trace solve (the fronts dominate;
+    per cell about 320 nd^2 log2(m) bytes in 2D and 40 nd^2 m^2 in 3D, nd the
+    trace dofs per face, fitted to the solver's own plans and rounded up)."""
+    nb = (k + 1) ** dim
+    nf = (k + 1) ** (dim - 1)
+    cells = m ** dim
+    Nt = 2 * dim * 3 * nf
+    Ns = 3 * nb
+    nd = 3 * nf
+    per_cell = 8 * (3 * (dim + 1) * nb * 3 + Nt * Nt + 3 * Nt + Ns * (1 + Nt))
+    if dim == 1:
+        fronts = 64 * nd * nd * cells
+    elif dim == 2:
+        fronts = 320 * nd * nd * max(math.log2(m), 1.0) * cells
+    else:
+        fronts = 40 * nd * nd * m * m * cells
+    return int(per_cell * cells + fronts + (64 << 20))
+
+
+def poisson_requests(n: int, rate: float, seed: int, sizes_2d=(32, 256), sizes_3d=(8, 16),
+                     degrees=(1, 2), frac_3d=0.25, bias=(0.0, 0.8)) -> list:
+    """n requests with exponential inter-arrival times (rate per second),
+    2D meshes uniform in sizes_2d, 3D meshes uniform in sizes_3d (degree 1),
+    degrees uniform in `degrees`, biases uniform in `bias`."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        if rng.random() < frac_3d:
+            dim, k = 3, 1
+            m = int(rng.integers(sizes_3d[0], sizes_3d[1] + 1))
+        else:
+            dim = 2
+            m = int(rng.integers(sizes_2d[0], sizes_2d[1] + 1))
+            k = int(rng.choice(degrees))
+        out.append(Request(i, dim, m, k, float(rng.uniform(*bias)), t))
+    return out
+
+
+def solve_one(req: Request, device="cuda:0", keep_state=False, tol=1e-10, max_it=50):
+    """One request's solve on the calling thread's current CUDA stream."""
+    from . import workloads
+    from .solver import NPSolver
+
+    pb, prm, adim = workloads.diode(dim=req.dim, m=req.m, k=req.k)
+    prm.consistent_drift_jacobian = True
+    prm.consistent_recombination_jacobian = True
+    g = NPSolver(pb, prm, adim, device=device)
+    res = g.compute_thermodynamic_equilibrium()
+    it = res.iterations
+    if req.bias != 0.0:
+        workloads.set_bias(pb, req.bias)
+        g.update_boundary_tables()
+        res = g.run(tol, tol, max_it)
+        it += res.iterations
+    state = (g.get_cell_state().copy(), g.get_trace_state().copy()) if keep_state else None
+    return res.converged, it, g.ncells, state
+
+
+class DiodeServer:
+    """Continuous batching of diode solves on one GPU.
+
+    max_inflight: requests on the device at once (slots).
+    hbm_reserve: bytes of device memory left free for everything else.
+    hbm_limit: treat the device as having at most this many bytes (tests)."""
+
+    def __init__(self, max_inflight=8, hbm_reserve=4 << 30, hbm_limit=None, device="cuda:0",
+                 keep_states=False):
+        self.max_inflight = max_inflight
+        self.hbm_reserve = hbm_reserve
+        self.hbm_limit = hbm_limit
+        self.device = device
+        self.keep_states = keep_states
+        self.peak_inflight = 0
+        self.peak_committed = 0  # largest sum of the in-flight requests' memory estimates
+
+    def _free_bytes(self, committed):
+        import torch
+
+        free, total = torch.cuda.mem_get_info(self.device)
+        if self.hbm_limit is not None:
+            free = min(free, self.hbm_limit - committed)
+        return free - self.hbm_reserve
+
+    def run(self, requests):
+        """Serve the requests (sorted by arrival time); returns their
+        results in request order.  Arrival times are honoured in wall-clock
+        time from the start of the call."""
+        import torch
+
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        results = {}
+        lock = threading.Lock()
+        done = threading.Condition(lock)
+        inflight = {}      # rid -> estimated bytes
+        committed = [0]
+        errors = []
+        t0 = time.perf_counter()
+
+        def worker(req, est, start):
+            try:
+                stream = torch.cuda.Stream(device=self.device)
+                with torch.cuda.stream(stream):
+                    conv, it, cells, state = solve_one(req, self.device, self.keep_states)
+                    stream.synchronize()
+                finish = time.perf_counter() - t0
+                res = Result(req.rid, req.arrival, start, finish, it, conv, cells, state)
+            except Exception as e:  # reported after the run
+                res = None
+                errors.append((req.rid, repr(e)))
+            with lock:
+                if res is not None:
+                    results[req.rid] = res
+                committed[0] -= est
+                del inflight[req.rid]
+                done.notify_all()
+
+        threads = []
+        i = 0
+        while i < len(reqs):
+            req = reqs[i]
+            now = time.perf_counter() - t0
+            if now < req.arrival:
+                time.sleep(min(req.arrival - now, 0.05))
+                continue
+            est = memory_estimate(req.dim, req.m, req.k)
+            with lock:
+                while inflight and (len(inflight) >= self.max_inflight or
+                                    est > self._free_bytes(committed[0])):
+                    done.wait(timeout=0.05)
+                if not inflight and est > self._free_bytes(committed[0]):
+                    errors.append((req.rid, "does not fit in device memory"))
+                    i += 1
+                    continue
+                inflight[req.rid] = est
+                committed[0] += est
+                self.peak_inflight = max(self.peak_inflight, len(inflight))
+                self.peak_committed = max(self.peak_committed, committed[0])
+            start = time.perf_counter() - t0
+            th = threading.Thread(target=worker, args=(req, est, start), daemon=True)
+            th.start()
+            threads.append(th)
+            i += 1
+        for th in threads:
+            th.join()
+        if errors:
+            raise RuntimeError(f"requests failed: {errors}")
+        return [results[r.rid] for r in requests]
+
+
+def latency_stats(results, wall):
+    lat = np.array([r.latency for r in results])
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "solves_per_s": len(results) / wall,
+            "cells_per_s": sum(r.cells for r in results) / wall,
+            "converged": int(sum(r.converged for r in results)), "requests": len(results)}

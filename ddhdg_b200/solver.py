@@ -421,7 +421,7 @@ class NPSolver:
                                              self.cell_state.data_ptr(), self._sp()), "project_cell")
         _lib.check(self.L.ddhdg_project_trace(self._ctx, dvt.data_ptr(), 0, self.trace_state.data_ptr(),
                                               self._sp()), "project_trace")
-        torch.cuda.synchronize(self.device)
+        self.stream.synchronize()
 
     def compute_thermodynamic_equilibrium(self, absolute_tol=None, relative_tol=None,
                                           max_number_of_iterations=None, generate_first_guess=True):
@@ -455,7 +455,7 @@ class NPSolver:
                                                  self.cell_state.data_ptr(), self._sp()), "project_cell")
             _lib.check(self.L.ddhdg_project_trace(self._ctx, torch.as_tensor(vt, device=self.device).data_ptr(),
                                                   c, self.trace_state.data_ptr(), self._sp()), "project_trace")
-            torch.cuda.synchronize(self.device)
+            self.stream.synchronize()
             return
         cs = self.get_cell_state()
         ts = self.get_trace_state()

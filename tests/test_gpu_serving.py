@@ -1,0 +1,50 @@
+"""Serving (continuous batching of diode solves on one GPU): every request's
+fields are the same alone and in the mix, requests really overlap, and the
+memory admission holds requests back when the device is full."""
+
+import numpy as np
+import pytest
+
+from ddhdg_b200 import serving
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests():
+    # sizes that the reference's (undamped) Newton solves at these biases:
+    # degree 2 needs cells of 1/32 um or less across the junction
+    spec = [(2, 16, 1, 0.3), (2, 20, 1, 0.5), (2, 32, 2, 0.8), (1, 64, 2, 0.6), (3, 4, 1, 0.1), (2, 32, 1, 0.2)]
+    return [serving.Request(i, d, m, k, b, 0.0) for i, (d, m, k, b) in enumerate(spec)]
+
+
+def test_results_are_the_same_alone_and_in_the_mix():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    reqs = _requests()
+    alone = serving.DiodeServer(max_inflight=1, keep_states=True).run(reqs)
+    mixed_server = serving.DiodeServer(max_inflight=4, keep_states=True)
+    mixed = mixed_server.run(reqs)
+    assert mixed_server.peak_inflight > 1
+    for a, b in zip(alone, mixed):
+        assert a.converged and b.converged
+        assert a.iterations == b.iterations
+        for x, y in zip(a.state, b.state):
+            assert np.array_equal(x, y), a.rid
+
+
+def test_memory_admission_limits_the_requests_in_flight():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    reqs = _requests()
+    biggest = max(serving.memory_estimate(r.dim, r.m, r.k) for r in reqs)
+    limit = 2 * biggest
+    server = serving.DiodeServer(max_inflight=8, hbm_reserve=0, hbm_limit=limit)
+    res = server.run(reqs)
+    assert all(r.converged for r in res)
+    assert server.peak_committed <= limit
+    total = sum(serving.memory_estimate(r.dim, r.m, r.k) for r in reqs)
+    assert server.peak_committed < total  # some requests had to wait
+    stats = serving.latency_stats(res, max(r.finish for r in res))
+    assert stats["p99_s"] >= stats["p50_s"] > 0
