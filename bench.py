@@ -221,6 +221,36 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_serve(args):
+    """The serving configuration: Poisson arrivals (seeded) of 2D (32^2..256^2)
+    and 3D (8^3..16^3, degree 1) diode solves, degrees 1-2, biases uniform in
+    0..0.8 V; continuous batching on one GPU (ddhdg_b200.serving)."""
+    import torch
+
+    from ddhdg_b200 import serving
+
+    torch.cuda.init()
+    # warm the library and the kernels once (not part of the stream)
+    serving.solve_one(serving.Request(-1, 2, 32, 1, 0.1, 0.0))
+    reqs = serving.poisson_requests(args.serve_requests, args.serve_rate, seed=2024)
+    server = serving.DiodeServer(max_inflight=8)
+    t0 = time.perf_counter()
+    res = server.run(reqs)
+    wall = time.perf_counter() - t0
+    st = serving.latency_stats(res, wall)
+    line = {"metric": "serve p50/p99 latency (diode solves, continuous batching)",
+            "value": st["p99_s"], "unit": "s", "higher_is_better": False, "n_gpus": 1, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "Poisson stream of 2D 32^2..256^2 (k 1-2) and 3D 8^3..16^3 (k 1) diode "
+                                   "solves, bias U[0, 0.8] V, equilibrium + warm-started Newton",
+                       "requests": len(reqs), "rate_per_s": args.serve_rate, "seed": 2024,
+                       "max_inflight": server.max_inflight},
+            "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"],
+            "solves_per_s": st["solves_per_s"], "cells_per_s": st["cells_per_s"],
+            "converged": st["converged"], "peak_inflight": server.peak_inflight, "wall_s": wall}
+    print(json.dumps(line))
+
+
 def run_bias_sweep(args):
     """The second diode configuration end to end: equilibrium, then a forward
     bias sweep 0.0..0.8 V in 0.05 V steps, each point warm-started, every
@@ -268,6 +298,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve", action="store_true",
+                    help="serve a seeded Poisson stream of diode solves and report p50/p99 latency")
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-rate", type=float, default=4.0, help="arrivals per second")
     ap.add_argument("--bias-sweep", action="store_true",
                     help="time the warm-started 0..0.8 V sweep (17 points) instead of the step")
     ap.add_argument("--cells-per-side", type=int, default=WORKLOAD["m"],
@@ -277,6 +311,8 @@ def main():
         return run_reference(args)
     if args.bias_sweep:
         return run_bias_sweep(args)
+    if args.serve:
+        return run_serve(args)
 
     import torch
     import torch.distributed as dist

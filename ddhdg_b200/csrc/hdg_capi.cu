@@ -1181,7 +1181,7 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
       if (r_global)
         {
           int per_sm = 0;
-          CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          CK(allow_full_dynamic_smem(cf.fn));
           CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, threads, smem));
           const int64_t g = std::min<int64_t>(units, (int64_t)std::max(per_sm, 1) * c->sm_count);
           if ((r = m.rscratch.alloc((size_t)g * c->nb * m.ncomp * m.ncol)))
@@ -1189,7 +1189,7 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
           P.rscratch = m.rscratch.p;
         }
     }
-  CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(allow_full_dynamic_smem(cf.fn));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, threads, smem));
   if (per_sm < 1)
@@ -1246,7 +1246,7 @@ ddhdg_reconstruct(ddhdg_ctx *c, const double *cell_state, const double *trace_st
   const size_t smem =
     ((nPQ + 1) & ~(size_t)1) * sizeof(double) + (size_t)wpb * wsz * sizeof(double);
   P.wpb = wpb;
-  CK(cudaFuncSetAttribute(rf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(allow_full_dynamic_smem(reinterpret_cast<const void *>(rf)));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rf, wpb * 32, smem));
   const int64_t blocks_needed = (c->ncells + wpb - 1) / wpb;
@@ -1608,7 +1608,7 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
       threads = CondenseTPB;
       units   = c->ncells;
     }
-  CK(cudaFuncSetAttribute(cf.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(allow_full_dynamic_smem(cf.fn));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, threads, smem));
   if (per_sm < 1)

@@ -29,13 +29,45 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/ddhdg_b200.h"
 
 namespace ddhdg
 {
+  // A kernel's dynamic shared-memory limit is process-wide state.  It is set
+  // once per device to the opt-in maximum (minus the kernel's static shared
+  // memory) and never lowered, so that contexts launching one kernel with
+  // different sizes from several host threads cannot race on it.
+  inline cudaError_t
+  allow_full_dynamic_smem(const void *fn)
+  {
+    static std::mutex                                  mu;
+    static std::vector<std::pair<int, const void *>> done;
+    int                                                dev = 0;
+    cudaError_t                                        e   = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+      return e;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &d : done)
+      if (d.first == dev && d.second == fn)
+        return cudaSuccess;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, fn)) != cudaSuccess)
+      return e;
+    int optin = 0;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess)
+      return e;
+    if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  optin - (int)fa.sharedSizeBytes)) != cudaSuccess)
+      return e;
+    done.push_back({dev, fn});
+    return cudaSuccess;
+  }
+
   struct NDAsm
   {
     int64_t off;     // front of the node (doubles)
@@ -609,25 +641,10 @@ namespace ddhdg
           cublasSetStream(side_blas_[k], side_[k]);
           cusolverDnSetStream(side_dn_[k], side_[k]);
         }
-      size_t max_small = 0;
-      for (auto &b : batches_)
-        if (b.small)
-          max_small = std::max(max_small, small_smem(b.nE, b.nK));
-      if (max_small > 48 * 1024)
-        if (cudaFuncSetAttribute(nd_small_front_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)max_small) != cudaSuccess)
-          return bad(err, "front too large for the fused small-front kernel", DDHDG_SOLVER_ERROR);
-      int max_nE = 0;
-      for (auto &b : batches_)
-        max_nE = std::max(max_nE, b.nE);
-      if (max_nE * sizeof(double) > 48 * 1024)
-        if (cudaFuncSetAttribute(nd_rowperm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(max_nE * sizeof(double))) != cudaSuccess)
-          return bad(err, "front too large for the row permutation", DDHDG_SOLVER_ERROR);
-      if (max_nK_ * sizeof(double) > 48 * 1024)
-        if (cudaFuncSetAttribute(nd_backsolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(max_nK_ * sizeof(double))) != cudaSuccess)
-          return bad(err, "front too large for the back substitution", DDHDG_SOLVER_ERROR);
+      if (allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_front_kernel)) != cudaSuccess ||
+          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_rowperm_kernel)) != cudaSuccess ||
+          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_backsolve_kernel)) != cudaSuccess)
+        return bad(err, "cannot raise the shared-memory limit of the trace-solve kernels", DDHDG_CUDA_ERROR);
       nodes_info_ = (int)nodes_.size();
       built_      = true;
       return DDHDG_OK;
