@@ -630,6 +630,8 @@ namespace ddhdg
         return r;
       if (cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) != cudaSuccess)
         return bad(err, "cudaEventCreate failed", DDHDG_CUDA_ERROR);
+      if (cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking) != cudaSuccess)
+        return bad(err, "cudaStreamCreate failed", DDHDG_CUDA_ERROR);
       for (int k = 0; k < NSide; ++k)
         {
           if (cudaStreamCreateWithFlags(&side_[k], cudaStreamNonBlocking) != cudaSuccess ||
@@ -650,18 +652,86 @@ namespace ddhdg
       return DDHDG_OK;
     }
 
-    // numeric phase: x (global trace dofs) from the per-cell condensed blocks
+    // numeric phase: x (global trace dofs) from the per-cell condensed
+    // blocks.  The whole sequence (about 10 launches per batch) is captured
+    // in a CUDA graph on the second call with the same buffers and replayed
+    // after that; the check for singular fronts stays outside the graph.
     int
     solve(const double *tt, const double *rhs, const int32_t *dflag, const double *dval, int Nt,
           double *x, cudaStream_t s, int sm_count, std::string &err)
     {
       if (!built_)
         return bad(err, "nested-dissection solver not built");
+      if (Nt != M_.F * M_.nd)
+        return bad(err, "trace block size does not match the solver");
+      const Key k{tt, rhs, dflag, dval, x, sm_count};
+      int       r = DDHDG_OK;
+      if (graphs_ok_ && exec_ && k == key_)
+        {
+          if (cudaGraphLaunch(exec_, s) != cudaSuccess)
+            return bad(err, "cudaGraphLaunch failed", DDHDG_CUDA_ERROR);
+        }
+      else if (graphs_ok_ && k == key_ && !exec_)
+        {
+          // same buffers as the last (eager) call: capture, then launch
+          cudaGraph_t gph = nullptr;
+          if (cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            {
+              cudaGetLastError();
+              graphs_ok_ = false;
+              r          = enqueue(tt, rhs, dflag, dval, Nt, x, s, sm_count, err);
+            }
+          else
+            {
+              const int         rc = enqueue(tt, rhs, dflag, dval, Nt, x, cap_, sm_count, err);
+              const cudaError_t e  = cudaStreamEndCapture(cap_, &gph);
+              if (rc || e != cudaSuccess || !gph ||
+                  cudaGraphInstantiate(&exec_, gph, 0) != cudaSuccess)
+                {
+                  cudaGetLastError();
+                  exec_      = nullptr;
+                  graphs_ok_ = false; // this build cannot capture: stay eager
+                  r          = enqueue(tt, rhs, dflag, dval, Nt, x, s, sm_count, err);
+                }
+              else if (cudaGraphLaunch(exec_, s) != cudaSuccess)
+                r = bad(err, "cudaGraphLaunch failed", DDHDG_CUDA_ERROR);
+              if (gph)
+                cudaGraphDestroy(gph);
+            }
+        }
+      else
+        {
+          if (exec_)
+            cudaGraphExecDestroy(exec_);
+          exec_ = nullptr;
+          key_  = k;
+          r     = enqueue(tt, rhs, dflag, dval, Nt, x, s, sm_count, err);
+        }
+      if (r)
+        return r;
+      return check_info(s, err);
+    }
+
+  private:
+    struct Key
+    {
+      const void *tt, *rhs, *dflag, *dval, *x;
+      int         sm;
+      bool
+      operator==(const Key &o) const
+      {
+        return tt == o.tt && rhs == o.rhs && dflag == o.dflag && dval == o.dval && x == o.x && sm == o.sm;
+      }
+    };
+
+    // the numeric phase's launches on stream s (no host synchronisation)
+    int
+    enqueue(const double *tt, const double *rhs, const int32_t *dflag, const double *dval, int Nt,
+            double *x, cudaStream_t s, int sm_count, std::string &err)
+    {
       const auto   &M     = M_;
       const int64_t ndofs = M.nfaces * (int64_t)M.nd;
       const int     grid  = sm_count * 8;
-      if (Nt != M.F * M.nd)
-        return bad(err, "trace block size does not match the solver");
       cublasSetStream(blas_, s);
       cusolverDnSetStream(dn_, s);
       // row equilibration
@@ -753,7 +823,13 @@ namespace ddhdg
         }
       if (cudaGetLastError() != cudaSuccess)
         return bad(err, "nested-dissection kernel launch failed", DDHDG_CUDA_ERROR);
-      // singular fronts
+      return DDHDG_OK;
+    }
+
+    // singular fronts (outside any graph: a host read)
+    int
+    check_info(cudaStream_t s, std::string &err)
+    {
       std::vector<int> info(nodes_info_);
       if (cudaMemcpyAsync(info.data(), d_info_, nodes_info_ * sizeof(int), cudaMemcpyDeviceToHost, s) !=
             cudaSuccess ||
@@ -765,7 +841,6 @@ namespace ddhdg
       return DDHDG_OK;
     }
 
-  private:
     static constexpr int NSide = 8; // side streams for the large fronts
 
     struct Node
@@ -1024,6 +1099,14 @@ namespace ddhdg
       if (ev_fork_)
         cudaEventDestroy(ev_fork_);
       ev_fork_ = nullptr;
+      if (exec_)
+        cudaGraphExecDestroy(exec_);
+      exec_ = nullptr;
+      if (cap_)
+        cudaStreamDestroy(cap_);
+      cap_       = nullptr;
+      key_       = Key{};
+      graphs_ok_ = true;
       built_ = false;
     }
 
@@ -1059,5 +1142,9 @@ namespace ddhdg
     cudaEvent_t         ev_join_[NSide]   = {};
     cudaEvent_t         ev_fork_          = nullptr;
     int64_t             work_per_         = 1;
+    cudaStream_t        cap_              = nullptr; // stream the graph is captured on
+    cudaGraphExec_t     exec_             = nullptr;
+    Key                 key_{};
+    bool                graphs_ok_ = true;
   };
 } // namespace ddhdg
