@@ -427,6 +427,51 @@ def main():
     e2e_ms = replicas.max_over_ranks(e0.elapsed_time(e1), dev) / args.steps
     e2e_value = replicas.job_throughput(nc, e2e_ms)
 
+    # ---- the mixed-precision condensation (FP32 Jacobian, FP64 residuals)
+    # on the same diode and state, timed the same way
+    mixed = None
+    if 3 * (WORKLOAD["k"] + 1) ** WORKLOAD["dim"] <= 32:
+        pbm, prmm, adimm = cases.diode(dim=WORKLOAD["dim"], m=m_side, k=WORKLOAD["k"],
+                                       length=m_side / WORKLOAD["m"], precision=1)
+        gm = NPSolver(pbm, prmm, adimm, device=str(dev))
+        gm.set_state(g.get_cell_state(), g.get_trace_state())
+        spm = gm._sp()
+
+        def condense_m():
+            _lib.check(L.ddhdg_assemble_condense(gm._ctx, gm.cell_state.data_ptr(), gm.trace_state.data_ptr(),
+                                                 0, tt.data_ptr(), rhs.data_ptr(), dflag.data_ptr(),
+                                                 dval.data_ptr(), spm), "condense (mixed)")
+
+        def reconstruct_m():
+            _lib.check(L.ddhdg_reconstruct(gm._ctx, gm.cell_state.data_ptr(), gm.trace_state.data_ptr(),
+                                           dtrace.data_ptr(), dcell.data_ptr(), 0, spm), "reconstruct (mixed)")
+
+        for _ in range(max(args.warmup, 3)):
+            condense_m()
+            reconstruct_m()
+        torch.cuda.synchronize()
+        evm = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps)]
+        replicas.barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            evm[3 * i].record(gm.stream)
+            condense_m()
+            evm[3 * i + 1].record(gm.stream)
+            reconstruct_m()
+            evm[3 * i + 2].record(gm.stream)
+        torch.cuda.synchronize()
+        cm = float(np.mean([evm[3 * i].elapsed_time(evm[3 * i + 1]) for i in range(args.steps)]))
+        rm = float(np.mean([evm[3 * i + 1].elapsed_time(evm[3 * i + 2]) for i in range(args.steps)]))
+        cm = replicas.max_over_ranks(cm, dev)
+        mixed = {"condense_ms": cm, "reconstruct_ms": rm,
+                 "cells_per_s": replicas.job_throughput(nc, cm + rm),
+                 "condense_speedup_vs_fp64": float(np.mean(cond_ms)) / cm,
+                 "kernel": "condense3_kernel<2,2,float>",
+                 "precision": "FP32 Jacobian (local operators, Gauss-Jordan, Y, Schur operands; "
+                              "FP64 accumulation of the products), FP64 residuals, FP64 outputs"}
+        del gm
+        torch.cuda.empty_cache()
+
     # ---- one whole Newton step (BASELINE's second metric): assembly +
     # condensation, nested-dissection trace solve, reconstruction, norms and
     # update, state on the device.  The consistent Jacobian keeps the
@@ -490,6 +535,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "cells/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "newton_step": newton,
+            "mixed": mixed,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }

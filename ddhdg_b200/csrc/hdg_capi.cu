@@ -483,7 +483,7 @@ namespace
     put(C.xi, sizeof(C.xi) / sizeof(double), T.xi);
   }
 
-  template <int D, int K>
+  template <int D, int K, typename JT>
   void
   launch_condense(const Tables &T, const KParams &P, int grid, int threads, size_t smem,
                   cudaStream_t s)
@@ -492,39 +492,56 @@ namespace
       {
         CTab<D, K> C;
         fill_ctab(T, C);
-        condense3_kernel<D, K><<<grid, threads, smem, s>>>(P, C);
+        condense3_kernel<D, K, JT><<<grid, threads, smem, s>>>(P, C);
       }
     else
       condense2_kernel<D, K><<<grid, threads, smem, s>>>(P);
   }
 
+  // mixed: the FP32-Jacobian variant of the warp-per-cell kernel; false when
+  // the (dim, degree) has none (the caller rejects mixed precision there)
   template <int D, int K>
-  void
-  pick(CondenseKernel &cf, ReconstructFn &rf)
+  bool
+  pick(CondenseKernel &cf, ReconstructFn &rf, bool mixed)
   {
     // warp-per-cell register kernel when one lane can own one row of the
     // scalar system, CTA-per-cell shared-memory kernel otherwise
+    rf = reconstruct_kernel<D, K>;
     if constexpr (3 * Dims<D, K>::nb <= 32)
-      cf.fn = reinterpret_cast<const void *>(condense3_kernel<D, K>);
+      {
+        if (mixed)
+          {
+            cf.fn     = reinterpret_cast<const void *>(condense3_kernel<D, K, float>);
+            cf.launch = launch_condense<D, K, float>;
+          }
+        else
+          {
+            cf.fn     = reinterpret_cast<const void *>(condense3_kernel<D, K, double>);
+            cf.launch = launch_condense<D, K, double>;
+          }
+        return true;
+      }
     else
-      cf.fn = reinterpret_cast<const void *>(condense2_kernel<D, K>);
-    cf.launch = launch_condense<D, K>;
-    rf        = reconstruct_kernel<D, K>;
+      {
+        cf.fn     = reinterpret_cast<const void *>(condense2_kernel<D, K>);
+        cf.launch = launch_condense<D, K, double>;
+        return !mixed;
+      }
   }
 
   bool
-  kernels_for(int dim, int k, CondenseKernel &cf, ReconstructFn &rf)
+  kernels_for(int dim, int k, CondenseKernel &cf, ReconstructFn &rf, bool mixed = false)
   {
     switch (dim * 10 + k)
       {
-        case 11: pick<1, 1>(cf, rf); return true;
-        case 12: pick<1, 2>(cf, rf); return true;
-        case 13: pick<1, 3>(cf, rf); return true;
-        case 21: pick<2, 1>(cf, rf); return true;
-        case 22: pick<2, 2>(cf, rf); return true;
-        case 23: pick<2, 3>(cf, rf); return true;
-        case 31: pick<3, 1>(cf, rf); return true;
-        case 32: pick<3, 2>(cf, rf); return true;
+        case 11: return pick<1, 1>(cf, rf, mixed);
+        case 12: return pick<1, 2>(cf, rf, mixed);
+        case 13: return pick<1, 3>(cf, rf, mixed);
+        case 21: return pick<2, 1>(cf, rf, mixed);
+        case 22: return pick<2, 2>(cf, rf, mixed);
+        case 23: return pick<2, 3>(cf, rf, mixed);
+        case 31: return pick<3, 1>(cf, rf, mixed);
+        case 32: return pick<3, 2>(cf, rf, mixed);
         default: return false;
       }
   }
@@ -932,6 +949,15 @@ ddhdg_ctx_create(const ddhdg_problem_desc *d, ddhdg_ctx **out)
     return fail(DDHDG_BAD_ARG, "dim must be 1..3 and degree 1..3");
   if (d->dim == 3 && d->degree > 2)
     return fail(DDHDG_BAD_ARG, "3D supports degree 1 and 2");
+  if (d->precision != 0 && d->precision != 1)
+    return fail(DDHDG_BAD_ARG, "precision must be 0 (FP64) or 1 (mixed)");
+  {
+    int nb = 1;
+    for (int a = 0; a < d->dim; ++a)
+      nb *= d->degree + 1;
+    if (d->precision == 1 && 3 * nb > 32)
+      return fail(DDHDG_BAD_ARG, "mixed precision needs 3 (k+1)^d <= 32 (1D, 2D k <= 2, 3D k = 1)");
+  }
   for (int a = 0; a < d->dim; ++a)
     if (d->n[a] < 1 || !(d->h[a] > 0.))
       return fail(DDHDG_BAD_ARG, "bad mesh");
@@ -1140,7 +1166,8 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
   Mode      &m = c->mode[thermo];
   CondenseKernel cf;
   ReconstructFn rf;
-  if (!kernels_for(c->dim, c->k, cf, rf))
+  const bool mixed = c->desc.precision == 1;
+  if (!kernels_for(c->dim, c->k, cf, rf, mixed))
     return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
   KParams P     = make_params(c, thermo);
   P.cell_state  = cell_state;
@@ -1156,9 +1183,10 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
   if (3 * c->nb <= 32)
     {
       // warp per cell: as many warps per CTA as shared memory allows
-      const Ws3Off w   = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol);
+      // mixed: two CTAs per SM (the FP32 kernel is built for 128 registers)
+      const Ws3Off w   = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, mixed ? 4 : 8);
       const size_t per = (size_t)w.total * sizeof(double);
-      int          wpb = (int)std::min<size_t>(Condense3MaxWPB, (220 * 1024) / per);
+      int          wpb = (int)std::min<size_t>(Condense3MaxWPB, (mixed ? 110 : 220) * 1024 / per);
       if (wpb < 1)
         return fail(DDHDG_BAD_ARG, "the per-cell workspace does not fit in shared memory");
       P.wpb   = wpb;

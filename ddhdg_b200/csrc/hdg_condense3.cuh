@@ -77,8 +77,25 @@ namespace ddhdg
     int ldr; // row stride of R / Y (even: 16-byte aligned rows)
   };
 
+  // row stride, in elements, of the staged S^-1 for a Jacobian type of jb
+  // bytes: FP64 as above; FP32 = 4 mod 32 floats, for the same reason
+  __host__ __device__ constexpr int
+  sinv_stride_for(int nsmax, int jb)
+  {
+    if (jb == 8)
+      return sinv_stride(nsmax);
+    int kp = (nsmax + 3) / 4 * 4;
+    while (kp % 32 != 4)
+      ++kp;
+    return kp;
+  }
+
+  // Offsets in doubles.  The Jacobian arrays (coefficients of the linearised
+  // operators, S, R / Y, T and the trace-row weights) hold elements of jb
+  // bytes: 8 in the FP64 kernel, 4 in the mixed one; everything that carries
+  // a residual stays FP64.
   __host__ __device__ inline Ws3Off
-  ws3_layout(int dim, int nb, int nf, int ncomp, int ncol)
+  ws3_layout(int dim, int nb, int nf, int ncomp, int ncol, int jb = 8)
   {
     const int F = 2 * dim, nqc = nb, Fq = F * nf, nqf = nf;
     const int Ns = ncomp * nb, Nt = F * ncomp * nf;
@@ -89,6 +106,8 @@ namespace ddhdg
       p += (n + 1) & ~1;
       return r;
     };
+    // n Jacobian elements, rounded up to whole 16-byte pairs of doubles
+    auto take_j = [&take, jb](int n) { return take((n * jb + 7) / 8); };
     o.coef = take(3 * (dim + 1) * nb);
     o.lam  = take(F * 3 * nf);
     o.c0   = take(3 * nqc);
@@ -100,38 +119,40 @@ namespace ddhdg
     o.Wrc  = take(3 * dim * nqc);
     o.tau  = take(F * 3);
     o.bcs  = take(F * 3);
-    o.al   = take(9 * nqc);
-    o.be   = take(9 * nqc * dim);
-    o.ka   = take(9 * nqc);
-    o.ga   = take(9 * Fq);
-    o.rh   = take(9 * Fq);
-    o.ctc  = take(3 * Fq);
-    o.ctd  = take(3 * Fq);
+    o.al   = take_j(9 * nqc);
+    o.be   = take_j(9 * nqc * dim);
+    o.ka   = take_j(9 * nqc);
+    o.ga   = take_j(9 * Fq);
+    o.rh   = take_j(9 * Fq);
+    o.ctc  = take_j(3 * Fq);
+    o.ctd  = take_j(3 * Fq);
     o.r0   = take(3 * nqc);
     o.r1   = take(3 * nqc * dim);
     o.rf   = take(3 * Fq);
     const int dead_end = p;
     p     = 0;
-    o.Trs = take(Ns * Nt);
-    o.rA  = take(Nt * 3 * nqf);
-    o.rS  = take(Nt * nqf);
-    o.rD  = take(Nt * nqf);
+    o.Trs = take_j(Ns * Nt);
+    o.rA  = take_j(Nt * 3 * nqf);
+    o.rS  = take_j(Nt * nqf);
+    o.rD  = take_j(Nt * nqf);
     o.rZ  = take(Nt);
     o.H   = take(3 * Fq);
     p     = p > dead_end ? p : dead_end;
     {
       // staged S^-1 of the tensor-path Y = S^-1 R ([rows padded to 8][stride])
-      const int sv = (3 * nb + 7) / 8 * 8 * sinv_stride(3 * nb);
+      const int sv = ((3 * nb + 7) / 8 * 8 * sinv_stride_for(3 * nb, jb) * jb + 7) / 8;
       p            = p > sv ? p : sv;
       p            = (p + 1) & ~1;
     }
-    o.tcS  = take(3 * Fq);
-    o.tcW  = take(9 * Fq);
-    o.ttc  = take(3 * Fq);
+    o.tcS  = take_j(3 * Fq);
+    o.tcW  = take_j(9 * Fq);
+    o.ttc  = take_j(3 * Fq);
     o.rhsf = take(3 * Fq);
     o.Wrf  = take(3 * Fq);
-    o.ldr  = (ncol + 1) & ~1;
-    o.R    = take(Ns * o.ldr);
+    // R / Y rows: even in FP64 (16-byte rows); odd in FP32, so that one row
+    // per lane walks 32 different banks
+    o.ldr  = jb == 8 ? (ncol + 1) & ~1 : (ncol | 1);
+    o.R    = take_j(Ns * o.ldr);
     o.g    = take(Nt);
     o.dfl  = take(Nt);
     o.Yc   = take(Ns);
@@ -139,8 +160,33 @@ namespace ddhdg
     return o;
   }
 
-  template <int DIM, int K>
-  __global__ void __launch_bounds__(Condense3MaxWPB * 32, 1)
+  // 32-bit pivot key of |x|: the high word of an FP64 value (sign, exponent
+  // and 20 mantissa bits), the bits of an FP32 value
+  __device__ __forceinline__ unsigned
+  pivot_key_bits(double x)
+  {
+    return (unsigned)((unsigned long long)__double_as_longlong(fabs(x)) >> 32);
+  }
+  __device__ __forceinline__ unsigned
+  pivot_key_bits(float x)
+  {
+    return __float_as_uint(fabsf(x));
+  }
+  __device__ __forceinline__ void
+  store_pair(double *p, double a, double b)
+  {
+    *reinterpret_cast<double2 *>(p) = make_double2(a, b);
+  }
+  __device__ __forceinline__ void
+  store_pair(float *p, float a, float b)
+  {
+    *reinterpret_cast<float2 *>(p) = make_float2(a, b);
+  }
+
+  // JT: the Jacobian type (double: the FP64 kernel; float: the mixed kernel,
+  // see the note on precision below)
+  template <int DIM, int K, typename JT = double>
+  __global__ void __launch_bounds__(Condense3MaxWPB * 32, sizeof(JT) == 8 ? 1 : 2)
   condense3_kernel(const KParams P, const __grid_constant__ CTab<DIM, K> C)
   {
     using Dm            = Dims<DIM, K>;
@@ -183,18 +229,19 @@ namespace ddhdg
     const double *QW_c   = tb + P.to.QW_c;
     const double *QW_f   = tb + P.to.QW_f;
 
-    const Ws3Off wo = ws3_layout(DIM, nb, nf, ncomp, ncol);
+    const Ws3Off wo = ws3_layout(DIM, nb, nf, ncomp, ncol, (int)sizeof(JT));
     double      *ws = smem + warp * wo.total;
+    const auto   jp = [ws](int off) { return reinterpret_cast<JT *>(ws + off); };
     double *coef = ws + wo.coef, *lam = ws + wo.lam, *c0 = ws + wo.c0, *W0 = ws + wo.W0,
            *qc = ws + wo.qc, *c0f = ws + wo.c0f, *W0n = ws + wo.W0n, *tr0 = ws + wo.tr0,
            *Wrc = ws + wo.Wrc, *Wrf = ws + wo.Wrf, *taus = ws + wo.tau, *bcs = ws + wo.bcs,
-           *al = ws + wo.al, *be = ws + wo.be, *ka = ws + wo.ka, *ga = ws + wo.ga,
-           *rh = ws + wo.rh, *ctc = ws + wo.ctc, *ctd = ws + wo.ctd, *tcS = ws + wo.tcS,
-           *tcW = ws + wo.tcW, *ttc = ws + wo.ttc, *rhsf = ws + wo.rhsf, *r0 = ws + wo.r0,
-           *r1 = ws + wo.r1, *rf = ws + wo.rf, *R = ws + wo.R,
+           *rhsf = ws + wo.rhsf, *r0 = ws + wo.r0, *r1 = ws + wo.r1, *rf = ws + wo.rf,
            *gv = ws + wo.g, *dfl = ws + wo.dfl, *Yc = ws + wo.Yc;
-    double *Trs = ws + wo.Trs, *rA = ws + wo.rA, *rS = ws + wo.rS, *rD = ws + wo.rD,
-           *rZ = ws + wo.rZ, *Hs = ws + wo.H;
+    JT *al = jp(wo.al), *be = jp(wo.be), *ka = jp(wo.ka), *ga = jp(wo.ga), *rh = jp(wo.rh),
+       *ctc = jp(wo.ctc), *ctd = jp(wo.ctd), *tcS = jp(wo.tcS), *tcW = jp(wo.tcW),
+       *ttc = jp(wo.ttc), *R = jp(wo.R);
+    JT     *Trs = jp(wo.Trs), *rA = jp(wo.rA), *rS = jp(wo.rS), *rD = jp(wo.rD);
+    double *rZ = ws + wo.rZ, *Hs = ws + wo.H;
     const int ldr  = wo.ldr;
     const int colC = two ? 1 + Nt : 1; // combined trace columns of Y
 
@@ -619,14 +666,14 @@ namespace ddhdg
 #pragma unroll
               for (int fq = 0; fq < Fq; ++fq)
                 v += TLf[fq * nb + a] * rfp[fq];
-              R[lane * ldr] = v;
+              R[lane * ldr] = (JT)v;
             }
             // trace columns, one trial component at a time
             for (int cj = 0; cj < ncomp; ++cj)
               {
                 const int     pr  = bi * 3 + cmp_of(cj);
-                const double *kap = ka + pr * nqc;
-                const double *rhp = rh + pr * Fq;
+                const JT     *kap = ka + pr * nqc;
+                const JT     *rhp = rh + pr * Fq;
                 double        acc[Ft];
 #pragma unroll
                 for (int t = 0; t < Ft; ++t)
@@ -634,7 +681,7 @@ namespace ddhdg
 #pragma unroll
                 for (int q = 0; q < nqc; ++q)
                   {
-                    const double kq = kap[q];
+                    const double kq = (double)kap[q];
 #pragma unroll
                     for (int s = 0; s < DIM; ++s)
                       {
@@ -647,7 +694,7 @@ namespace ddhdg
 #pragma unroll
                 for (int fq = 0; fq < Fq; ++fq)
                   {
-                    const double w = rhp[fq] * TLf[fq * nb + a];
+                    const double w = (double)rhp[fq] * TLf[fq * nb + a];
 #pragma unroll
                     for (int t = 0; t < Ft; ++t)
                       acc[t] -= w * C.RQr[fq * Ft + t];
@@ -660,7 +707,7 @@ namespace ddhdg
                       for (int qf = 0; qf < nqf; ++qf)
                         {
                           const int    fq = f * nqf + qf;
-                          const double w  = ctc[bi * Fq + fq] * TLf[fq * nb + a];
+                          const double w  = (double)ctc[bi * Fq + fq] * TLf[fq * nb + a];
 #pragma unroll
                           for (int m = 0; m < nf; ++m)
                             acc[f * nf + m] += w * C.xi[qf * nf + m];
@@ -670,7 +717,7 @@ namespace ddhdg
                 for (int f = 0; f < F; ++f)
 #pragma unroll
                   for (int m = 0; m < nf; ++m)
-                    R[lane * ldr + 1 + (f * ncomp + cj) * nf + m] = acc[f * nf + m];
+                    R[lane * ldr + 1 + (f * ncomp + cj) * nf + m] = (JT)acc[f * nf + m];
                 if (two)
                   {
                     // drift columns are only used added to the trace columns:
@@ -686,9 +733,9 @@ namespace ddhdg
                             for (int qf = 0; qf < nqf; ++qf)
                               {
                                 const int fq = f * nqf + qf;
-                                d += ctd[bi * Fq + fq] * TLf[fq * nb + a] * C.xi[qf * nf + m];
+                                d += (double)ctd[bi * Fq + fq] * TLf[fq * nb + a] * C.xi[qf * nf + m];
                               }
-                          R[lane * ldr + 1 + Nt + (f * ncomp + cj) * nf + m] = d;
+                          R[lane * ldr + 1 + Nt + (f * ncomp + cj) * nf + m] = (JT)d;
                         }
                   }
               }
@@ -697,21 +744,21 @@ namespace ddhdg
         // ------------ S row per lane, in-place Gauss-Jordan inverse
         // lanes Ns..NSMAX-1 carry unit rows, so that the elimination always
         // runs over NSMAX columns (S padded to diag(S, I))
-        double srow[NSMAX];
+        JT srow[NSMAX];
 #pragma unroll
         for (int j = 0; j < NSMAX; ++j)
-          srow[j] = (lane >= Ns && lane == j) ? 1. : 0.;
+          srow[j] = (lane >= Ns && lane == j) ? JT(1) : JT(0);
         if (act)
           {
 #pragma unroll 1
             for (int cj = 0; cj < ncomp; ++cj)
               {
                 const int     pr  = bi * 3 + cmp_of(cj);
-                const double *alp = al + pr * nqc;
-                const double *kap = ka + pr * nqc;
-                const double *bep = be + pr * nqc * DIM;
-                const double *gap = ga + pr * Fq;
-                const double *rhp = rh + pr * Fq;
+                const JT     *alp = al + pr * nqc;
+                const JT     *kap = ka + pr * nqc;
+                const JT     *bep = be + pr * nqc * DIM;
+                const JT     *gap = ga + pr * Fq;
+                const JT     *rhp = rh + pr * Fq;
                 double        acc[nb];
 #pragma unroll
                 for (int e = 0; e < nb; ++e)
@@ -719,14 +766,14 @@ namespace ddhdg
 #pragma unroll
                 for (int q = 0; q < nqc; ++q)
                   {
-                    double lt = alp[q] * TLc[q * nb + a];
+                    double lt = (double)alp[q] * TLc[q * nb + a];
                     double kt[DIM];
 #pragma unroll
                     for (int s = 0; s < DIM; ++s)
                       {
                         const double tg = TLg[(q * DIM + s) * nb + a];
-                        lt += bep[q * DIM + s] * tg;
-                        kt[s] = kap[q] * tg;
+                        lt += (double)bep[q * DIM + s] * tg;
+                        kt[s] = (double)kap[q] * tg;
                       }
 #pragma unroll
                     for (int e = 0; e < nb; ++e)
@@ -741,7 +788,7 @@ namespace ddhdg
                 for (int fq = 0; fq < Fq; ++fq)
                   {
                     const double tf = TLf[fq * nb + a];
-                    const double g_ = gap[fq] * tf, r_ = rhp[fq] * tf;
+                    const double g_ = (double)gap[fq] * tf, r_ = (double)rhp[fq] * tf;
 #pragma unroll
                     for (int e = 0; e < nb; ++e)
                       acc[e] += g_ * C.phi_f[fq * nb + e] + r_ * C.RTr[fq * nb + e];
@@ -750,20 +797,20 @@ namespace ddhdg
 #pragma unroll
                 for (int k = 0; k < NSMAX; ++k)
                   if (k / nb == cj)
-                    srow[k] = acc[k % nb];
+                    srow[k] = (JT)acc[k % nb];
               }
           }
         // ---------------------------------------- Gauss-Jordan inverse
         // Row equilibration: S' = D S with D = diag(1/max|row|).  The sweep
         // below inverts S'; S^-1 = S'^-1 D, so column k of the inverse is
         // scaled by the factor of row p_k before it multiplies R.
-        double rscale;
+        JT rscale;
         {
-          double mx = 0.;
+          JT mx = 0;
 #pragma unroll
           for (int j = 0; j < NSMAX; ++j)
             mx = fmax(mx, fabs(srow[j]));
-          rscale = (mx > 0.) ? 1. / mx : 1.;
+          rscale = (mx > JT(0)) ? JT(1) / mx : JT(1);
 #pragma unroll
           for (int j = 0; j < NSMAX; ++j)
             srow[j] *= rscale;
@@ -780,7 +827,7 @@ namespace ddhdg
         // largest candidate, ties go to the lowest lane.  The pivot row is
         // broadcast through shared memory (the coefficient block, dead here).
         static_assert(NSMAX < 32, "key 0 marks used lanes");
-        double *prow  = coef;
+        JT     *prow  = reinterpret_cast<JT *>(coef);
         bool    used  = lane >= NSMAX;
         int     mypos = 0;
         bool    sing  = false;
@@ -790,8 +837,7 @@ namespace ddhdg
             unsigned key = 0u;
             if (!used)
               {
-                const unsigned hi =
-                  (unsigned)((unsigned long long)__double_as_longlong(fabs(srow[0])) >> 32);
+                const unsigned hi = pivot_key_bits(srow[0]);
                 key = (hi & ~31u) | (31u - (unsigned)lane);
               }
             const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
@@ -801,18 +847,17 @@ namespace ddhdg
               {
 #pragma unroll
                 for (int k = 0; k < NSMAX; k += 2)
-                  reinterpret_cast<double2 *>(prow)[k / 2] =
-                    make_double2(srow[k], k + 1 < NSMAX ? srow[k + 1] : 0.);
+                  store_pair(prow + k, srow[k], k + 1 < NSMAX ? srow[k + 1] : JT(0));
               }
             __syncwarp();
-            const double pj = prow[0];
+            const JT pj = prow[0];
             sing |= kmax < 32u || !isfinite(pj);
-            const double hr = (pj != 0.) ? 1. / pj : 0.;
-            const double l  = srow[0] * hr;
+            const JT hr = (pj != JT(0)) ? JT(1) / pj : JT(0);
+            const JT l  = srow[0] * hr;
 #pragma unroll
             for (int k = 1; k < NSMAX; ++k)
               {
-                const double pk = prow[k];
+                const JT pk = prow[k];
                 srow[k - 1]     = me ? -pk * hr : srow[k] - l * pk;
               }
             srow[NSMAX - 1] = me ? hr : l;
@@ -830,7 +875,7 @@ namespace ddhdg
         __syncwarp();
         // fold the row scaling of equation p_k into column k
         {
-          double dsc[NSMAX];
+          JT dsc[NSMAX];
 #pragma unroll
           for (int k = 0; k < NSMAX; ++k)
             dsc[k] = __shfl_sync(0xffffffffu, rscale, piv3[warp][k]);
@@ -843,8 +888,8 @@ namespace ddhdg
         {
           constexpr int MP = (NSMAX + 7) / 8 * 8;
           constexpr int KP = (NSMAX + 3) / 4 * 4;
-          constexpr int KS = sinv_stride(NSMAX);
-          double       *Sv = coef; // the coefficient block is dead here
+          constexpr int KS = sinv_stride_for(NSMAX, (int)sizeof(JT));
+          JT           *Sv = reinterpret_cast<JT *>(coef); // the coefficient block is dead here
           for (int idx = lane; idx < MP * KS; idx += 32)
             Sv[idx] = 0.;
           __syncwarp();
@@ -864,7 +909,7 @@ namespace ddhdg
               for (int ks = 0; ks < KP / 4; ++ks)
                 {
                   const int kk = ks * 4 + tq;
-                  bf[ks]       = (kk < Ns && col < ncol) ? R[piv3[warp][kk] * ldr + col] : 0.;
+                  bf[ks] = (kk < Ns && col < ncol) ? (double)R[piv3[warp][kk] * ldr + col] : 0.;
                 }
               double acc[MP / 8][2];
 #pragma unroll
@@ -873,7 +918,8 @@ namespace ddhdg
                   acc[mt][0] = acc[mt][1] = 0.;
 #pragma unroll
                   for (int ks = 0; ks < KP / 4; ++ks)
-                    dmma8x8x4(acc[mt][0], acc[mt][1], Sv[(mt * 8 + g) * KS + ks * 4 + tq], bf[ks]);
+                    dmma8x8x4(acc[mt][0], acc[mt][1], (double)Sv[(mt * 8 + g) * KS + ks * 4 + tq],
+                              bf[ks]);
                 }
               __syncwarp(); // every lane has read this block of R columns
 #pragma unroll
@@ -885,13 +931,13 @@ namespace ddhdg
                     {
                       const int c = n0 + 2 * tq + e;
                       if (row < Ns && c < ncol)
-                        R[row * ldr + c] = acc[mt][e];
+                        R[row * ldr + c] = (JT)acc[mt][e];
                     }
                 }
               __syncwarp();
             }
         }
-        double *const Y = R;
+        JT *const Y = R;
 
         // ------------------------ keep Y for the reconstruction [col][row]
         {
@@ -1048,7 +1094,7 @@ namespace ddhdg
                 continue;
               const int  fi  = i / (ncomp * nf), ci2 = (i / nf) % ncomp;
               const bool rok = dfl[i] == 0.;
-              const double *rAi = rA + i * 3 * nqf, *rDi = rD + i * nqf;
+              const JT    *rAi = rA + i * 3 * nqf, *rDi = rD + i * nqf;
 #pragma unroll
               for (int nt = 0; nt < NNT; ++nt)
 #pragma unroll
