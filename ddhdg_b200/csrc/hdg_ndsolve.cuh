@@ -182,28 +182,56 @@ namespace ddhdg
       }
   }
 
-  // x_E = y_E - W x_K for every node of a batch; CTA (node, block of 256
-  // eliminated rows)
+  // x_E = y_E - W x_K for every node of a batch.  CTA (node, block of R
+  // eliminated rows) of R x S threads: thread (row t % R, slice t / R) sums
+  // the terms k = slice, slice + S, ... of W x_K (for one k the R rows are
+  // consecutive in memory), and the S partial sums of a row are added in
+  // shared memory.  Short dependency chains: the top fronts have few rows per
+  // node and thousands of kept dofs.
   __global__ void
-  nd_backsolve_kernel(int nF, int nE, const NDSol *nodes, const int32_t *fdofs,
+  nd_backsolve_kernel(int nF, int nE, int R, const NDSol *nodes, const int32_t *fdofs,
                       const double *fronts, double *x)
   {
-    extern __shared__ double xk[];
-    const NDSol    n  = nodes[blockIdx.x];
-    const int      nK = nF - nE;
-    const int32_t *dl = fdofs + n.doff;
+    extern __shared__ double sh[];
+    const NDSol    n    = nodes[blockIdx.x];
+    const int      nK   = nF - nE;
+    const int      S    = blockDim.x / R;
+    double        *xk   = sh;
+    double        *part = sh + nK;
+    const int32_t *dl   = fdofs + n.doff;
     for (int k = threadIdx.x; k < nK; k += blockDim.x)
       xk[k] = x[dl[nE + k]];
     __syncthreads();
     const double *Fv = fronts + n.off;
-    const int     i  = blockIdx.y * blockDim.x + threadIdx.x;
-    if (i < nE)
+    const int     t  = threadIdx.x, il = t % R, sl = t / R;
+    const int     i  = blockIdx.y * R + il;
+    if (sl < S)
+      {
+        double v = 0.;
+        if (i < nE)
+          for (int k = sl; k < nK; k += S)
+            v += Fv[(int64_t)(nE + k) * nF + i] * xk[k];
+        part[sl * R + il] = v;
+      }
+    __syncthreads();
+    if (t < R && i < nE)
       {
         double v = Fv[(int64_t)nF * nF + i];
-        for (int k = 0; k < nK; ++k)
-          v -= Fv[(int64_t)(nE + k) * nF + i] * xk[k];
+        for (int q = 0; q < S; ++q)
+          v -= part[q * R + t];
         x[dl[i]] = v;
       }
+  }
+
+  // rows per CTA and slices of the kept dofs of the back substitution of a
+  // batch (R x S <= 1024 threads, about 8 or more terms per thread)
+  inline void
+  nd_backsolve_shape(int nE, int nK, int &R, int &S)
+  {
+    R = nE < 32 ? nE : 32;
+    S = (nK + 7) / 8;
+    S = S < 1 ? 1 : S;
+    S = S > 1024 / R ? 1024 / R : S;
   }
 
   // row permutation of a batch's LU factorisations: the sequential swaps of
@@ -405,6 +433,219 @@ namespace ddhdg
       info[blockIdx.x] = sing_s;
   }
 
+  // Mid fronts (NDSmallE < nE <= NDMidE), one CTA of 16 warps per front
+  // (above 72 eliminated dofs the single-warp diagonal-block solves make it
+  // slower than the batched cuBLAS path):
+  // - LU of F_EE with partial pivoting in shared memory (row swaps in shared
+  //   memory, the permutation kept as perm[i] = source row of row i);
+  // - W = U^-1 L^-1 P [F_EK | r_E] in chunks of NDMidCols columns, staged in
+  //   shared memory row-major (stride NDMidCols + 1: conflict-free by rows
+  //   and by columns) with the permutation applied on the load: blocked
+  //   triangular solves, each diagonal block of NDMidNB rows solved by one
+  //   warp in registers (a lane per column), the rows beyond it updated by
+  //   all warps (a warp per row, a lane per column);
+  // - the chunk written back to the front over [F_EK | r_E].
+  // The Schur update F_KK -= F_KE W follows as a batched GEMM.
+  // info[front] = first zero pivot (1-based) or 0.
+  constexpr int NDMidE    = 72;
+  constexpr int NDMidCols = 32;
+  constexpr int NDMidLdb  = NDMidCols + 1;
+  constexpr int NDMidNB   = 16;
+  constexpr int NDMidTPB  = 512;
+
+  __host__ __device__ inline size_t
+  nd_mid_smem(int nE)
+  {
+    return ((size_t)nE * nE + (size_t)nE * NDMidLdb + nE) * sizeof(double) + (size_t)nE * sizeof(int);
+  }
+
+  __global__ void __launch_bounds__(NDMidTPB)
+  nd_mid_front_kernel(int nE, int nK, const NDSol *nodes, int *info, double *fronts)
+  {
+    extern __shared__ double sm[];
+    __shared__ int     piv_s, sing_s;
+    constexpr int      NW = NDMidTPB / 32;
+    const int          nF = nE + nK, nc = nK + 1;
+    double            *A    = sm;                // [nE][nE] column-major
+    double            *Bc   = A + nE * nE;       // [nE][NDMidLdb] row-major
+    double            *dinv = Bc + nE * NDMidLdb;
+    int               *perm = reinterpret_cast<int *>(dinv + nE);
+    double            *Fv   = fronts + nodes[blockIdx.x].off;
+    const int          tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int c = warp; c < nE; c += NW)
+      for (int i = lane; i < nE; i += 32)
+        A[i + c * nE] = Fv[(int64_t)c * nF + i];
+    for (int i = tid; i < nE; i += NDMidTPB)
+      perm[i] = i;
+    if (tid == 0)
+      sing_s = 0;
+    __syncthreads();
+    // ------------------------------------------------------------ LU of F_EE
+    for (int j = 0; j < nE; ++j)
+      {
+        if (warp == 0)
+          {
+            double best = -1.;
+            int    bi   = nE;
+            for (int i = j + lane; i < nE; i += 32)
+              {
+                const double v = fabs(A[i + j * nE]);
+                if (v > best)
+                  {
+                    best = v;
+                    bi   = i;
+                  }
+              }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+              {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int    oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi))
+                  {
+                    best = ob;
+                    bi   = oi;
+                  }
+              }
+            if (lane == 0)
+              {
+                const int p = (bi < nE) ? bi : j;
+                piv_s       = p;
+                const int t = perm[j];
+                perm[j]     = perm[p];
+                perm[p]     = t;
+                if (!(best > 0.) || !isfinite(best))
+                  if (sing_s == 0)
+                    sing_s = j + 1;
+              }
+          }
+        __syncthreads();
+        const int p = piv_s;
+        if (p != j)
+          for (int c = tid; c < nE; c += NDMidTPB)
+            {
+              const double t = A[j + c * nE];
+              A[j + c * nE]  = A[p + c * nE];
+              A[p + c * nE]  = t;
+            }
+        __syncthreads();
+        const double d  = A[j + j * nE];
+        const double hr = (d != 0.) ? 1. / d : 0.;
+        if (tid == 0)
+          dinv[j] = hr;
+        for (int i = j + 1 + tid; i < nE; i += NDMidTPB)
+          A[i + j * nE] *= hr;
+        __syncthreads();
+        for (int c = j + 1 + warp; c < nE; c += NW)
+          {
+            const double ajc = A[j + c * nE];
+            for (int i = j + 1 + lane; i < nE; i += 32)
+              A[i + c * nE] -= A[i + j * nE] * ajc;
+          }
+        __syncthreads();
+      }
+    // ------------------------------------------- W, NDMidCols columns at a time
+    const int nblk = (nE + NDMidNB - 1) / NDMidNB;
+    for (int c0 = 0; c0 < nc; c0 += NDMidCols)
+      {
+        const int w = min(NDMidCols, nc - c0);
+        for (int c = warp; c < w; c += NW)
+          for (int i = lane; i < nE; i += 32)
+            Bc[i * NDMidLdb + c] = Fv[(int64_t)(nE + c0 + c) * nF + perm[i]];
+        __syncthreads();
+        // unit lower triangle, block by block
+        for (int kb = 0; kb < nE; kb += NDMidNB)
+          {
+            const int kn = min(NDMidNB, nE - kb);
+            if (warp == 0 && lane < w)
+              {
+                double x[NDMidNB];
+#pragma unroll
+                for (int r = 0; r < NDMidNB; ++r)
+                  x[r] = (r < kn) ? Bc[(kb + r) * NDMidLdb + lane] : 0.;
+#pragma unroll
+                for (int r = 0; r < NDMidNB; ++r)
+#pragma unroll
+                  for (int q = r + 1; q < NDMidNB; ++q)
+                    if (q < kn)
+                      x[q] -= A[(kb + q) + (kb + r) * nE] * x[r];
+#pragma unroll
+                for (int r = 0; r < NDMidNB; ++r)
+                  if (r < kn)
+                    Bc[(kb + r) * NDMidLdb + lane] = x[r];
+              }
+            __syncthreads();
+            if (kb + kn < nE && lane < w)
+              {
+                double x[NDMidNB];
+#pragma unroll
+                for (int r = 0; r < NDMidNB; ++r)
+                  x[r] = (r < kn) ? Bc[(kb + r) * NDMidLdb + lane] : 0.;
+                for (int i = kb + kn + warp; i < nE; i += NW)
+                  {
+                    double acc = 0.;
+#pragma unroll
+                    for (int r = 0; r < NDMidNB; ++r)
+                      if (r < kn)
+                        acc += A[i + (kb + r) * nE] * x[r];
+                    Bc[i * NDMidLdb + lane] -= acc;
+                  }
+              }
+            __syncthreads();
+          }
+        // upper triangle, block by block from the last
+        for (int bq = nblk - 1; bq >= 0; --bq)
+          {
+            const int kb = bq * NDMidNB;
+            const int kn = min(NDMidNB, nE - kb);
+            if (warp == 0 && lane < w)
+              {
+                double x[NDMidNB];
+#pragma unroll
+                for (int r = 0; r < NDMidNB; ++r)
+                  x[r] = (r < kn) ? Bc[(kb + r) * NDMidLdb + lane] : 0.;
+#pragma unroll
+                for (int r = NDMidNB - 1; r >= 0; --r)
+                  if (r < kn)
+                    {
+                      x[r] *= dinv[kb + r];
+#pragma unroll
+                      for (int q = 0; q < r; ++q)
+                        x[q] -= A[(kb + q) + (kb + r) * nE] * x[r];
+                    }
+#pragma unroll
+                for (int r = 0; r < NDMidNB; ++r)
+                  if (r < kn)
+                    Bc[(kb + r) * NDMidLdb + lane] = x[r];
+              }
+            __syncthreads();
+            if (kb > 0 && lane < w)
+              {
+                double x[NDMidNB];
+#pragma unroll
+                for (int r = 0; r < NDMidNB; ++r)
+                  x[r] = (r < kn) ? Bc[(kb + r) * NDMidLdb + lane] : 0.;
+                for (int i = warp; i < kb; i += NW)
+                  {
+                    double acc = 0.;
+#pragma unroll
+                    for (int r = 0; r < NDMidNB; ++r)
+                      if (r < kn)
+                        acc += A[i + (kb + r) * nE] * x[r];
+                    Bc[i * NDMidLdb + lane] -= acc;
+                  }
+              }
+            __syncthreads();
+          }
+        for (int c = warp; c < w; c += NW)
+          for (int i = lane; i < nE; i += 32)
+            Fv[(int64_t)(nE + c0 + c) * nF + i] = Bc[i * NDMidLdb + c];
+        __syncthreads();
+      }
+    if (tid == 0)
+      info[blockIdx.x] = sing_s;
+  }
+
   // -------------------------------------------------------------- host side
   class NDSolver
   {
@@ -576,6 +817,7 @@ namespace ddhdg
               }
           b.big   = b.nE >= 384 && b.nodes.size() <= 32;
           b.small = !b.big && b.nE > 0 && b.nE <= NDSmallE && small_smem(b.nE, b.nK) <= 200 * 1024;
+          b.mid   = !b.big && !b.small && b.nE > 0 && b.nE <= NDMidE && nd_mid_smem(b.nE) <= 220 * 1024;
           max_nK_ = std::max(max_nK_, b.nK);
         }
       return DDHDG_OK;
@@ -645,7 +887,8 @@ namespace ddhdg
         }
       if (allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_front_kernel)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_rowperm_kernel)) != cudaSuccess ||
-          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_backsolve_kernel)) != cudaSuccess)
+          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_backsolve_kernel)) != cudaSuccess ||
+          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_mid_front_kernel)) != cudaSuccess)
         return bad(err, "cannot raise the shared-memory limit of the trace-solve kernels", DDHDG_CUDA_ERROR);
       nodes_info_ = (int)nodes_.size();
       built_      = true;
@@ -781,6 +1024,20 @@ namespace ddhdg
                   info_base += nb;
                   continue;
                 }
+              if (b.mid)
+                {
+                  nd_mid_front_kernel<<<nb, NDMidTPB, nd_mid_smem(b.nE), s>>>(b.nE, b.nK, d_sol_ + b.sol_off,
+                                                                             inf, d_fronts_);
+                  if (b.nK > 0)
+                    {
+                      const double mone = -1., one = 1.;
+                      if (cublasDgemmBatched(blas_, CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE, &mone,
+                                             pKE, nF, pEK, nF, &one, pKK, nF, nb) != CUBLAS_STATUS_SUCCESS)
+                        return bad(err, "cublasDgemmBatched failed", DDHDG_SOLVER_ERROR);
+                    }
+                  info_base += nb;
+                  continue;
+                }
               if (cublasDgetrfBatched(blas_, b.nE, pEE, nF, piv, inf, nb) != CUBLAS_STATUS_SUCCESS)
                 return bad(err, "cublasDgetrfBatched failed", DDHDG_SOLVER_ERROR);
               // W = U^-1 L^-1 P [F_EK | r_E]: the row permutation by a
@@ -817,9 +1074,11 @@ namespace ddhdg
           if (b.nE == 0)
             continue;
           const int nF = b.nE + b.nK;
-          const dim3 g2((unsigned)b.nodes.size(), (b.nE + 255) / 256);
-          nd_backsolve_kernel<<<g2, 256, b.nK * sizeof(double), s>>>(nF, b.nE, d_sol_ + b.sol_off,
-                                                                     d_fdofs_, d_fronts_, x);
+          int       R, S;
+          nd_backsolve_shape(b.nE, b.nK, R, S);
+          const dim3 g2((unsigned)b.nodes.size(), (b.nE + R - 1) / R);
+          nd_backsolve_kernel<<<g2, R * S, (size_t)(b.nK + R * S) * sizeof(double), s>>>(
+            nF, b.nE, R, d_sol_ + b.sol_off, d_fdofs_, d_fronts_, x);
         }
       if (cudaGetLastError() != cudaSuccess)
         return bad(err, "nested-dissection kernel launch failed", DDHDG_CUDA_ERROR);
@@ -862,6 +1121,7 @@ namespace ddhdg
       bool             big     = false;
       int              maxc[2] = {0, 0}; // max child nK + 1 per extend-add pass
       bool             small   = false;  // fused one-CTA elimination
+      bool             mid     = false;  // one-CTA LU + W, batched GEMM Schur update
     };
 
     static size_t
