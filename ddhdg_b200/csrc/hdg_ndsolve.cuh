@@ -155,30 +155,33 @@ namespace ddhdg
   }
 
   // extend-add of child s's Schur complement (kept rows/columns and the rhs
-  // column) into the node's front: CTA (node, block of NDAsmCols child
-  // columns).  The two children are added by two launches, one after the
-  // other (they overlap on the split-plane block).
-  constexpr int NDAsmCols = 8;
+  // column) into the node's front: CTA (node, range of `per` elements, at
+  // least NDAsmElems, of the child's (cnK + 1) x cnK block, column-major),
+  // one element per thread and step, so that the reads are coalesced over
+  // the child's rows and every thread has work even for the few kept dofs of
+  // the low fronts.
+  // The two children are added by two launches, one after the other (they
+  // overlap on the split-plane block).
+  constexpr int NDAsmElems = 2048;
 
   __global__ void
-  nd_assemble_kernel(int nF, int s, const NDAsm *nodes, const int32_t *emap, double *fronts)
+  nd_assemble_kernel(int nF, int s, int64_t per, const NDAsm *nodes, const int32_t *emap, double *fronts)
   {
     const NDAsm    nd  = nodes[blockIdx.x];
     const int      cnF = nd.cnF[s], cnE = nd.cnE[s], cnK = cnF - cnE;
-    const int      j0  = blockIdx.y * NDAsmCols;
-    if (j0 > cnK)
+    const int64_t  tot = (int64_t)(cnK + 1) * cnK;
+    const int64_t  e0  = (int64_t)blockIdx.y * per;
+    if (e0 >= tot)
       return;
+    const int64_t  e1  = e0 + per < tot ? e0 + per : tot;
     double        *Fv  = fronts + nd.off;
     const double  *Fc  = fronts + nd.coff[s];
     const int32_t *map = emap + nd.moff[s];
-    const int      j1  = min(cnK + 1, j0 + NDAsmCols);
-    for (int j = j0; j < j1; ++j)
+    for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x)
       {
-        const int     pj = (j < cnK) ? map[j] : nF;
-        const double *cj = Fc + (int64_t)(cnE + j) * cnF + cnE;
-        double       *vj = Fv + (int64_t)pj * nF;
-        for (int i = threadIdx.x; i < cnK; i += blockDim.x)
-          vj[map[i]] += cj[i];
+        const int j  = (int)(e / cnK), i = (int)(e - (int64_t)j * cnK);
+        const int pj = (j < cnK) ? map[j] : nF;
+        Fv[(int64_t)pj * nF + map[i]] += Fc[(int64_t)(cnE + j) * cnF + cnE + i];
       }
   }
 
@@ -1000,8 +1003,13 @@ namespace ddhdg
                 return bad(err, "memset failed", DDHDG_CUDA_ERROR);
               for (int c = 0; c < 2; ++c)
                 {
-                  const dim3 g2(nb, (b.maxc[c] + NDAsmCols - 1) / NDAsmCols);
-                  nd_assemble_kernel<<<g2, 256, 0, s>>>(nF, c, d_asm_ + b.asm_off, d_emap_, d_fronts_);
+                  const int64_t ck = b.maxc[c] - 1; // largest child nK of this pass
+                  if (ck <= 0)
+                    continue;
+                  const int64_t tot = (ck + 1) * ck;
+                  const int64_t per = std::max<int64_t>(NDAsmElems, (tot + 65534) / 65535);
+                  const dim3    g2(nb, (unsigned)((tot + per - 1) / per));
+                  nd_assemble_kernel<<<g2, 256, 0, s>>>(nF, c, per, d_asm_ + b.asm_off, d_emap_, d_fronts_);
                 }
             }
           if (b.nE > 0)
