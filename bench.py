@@ -291,6 +291,121 @@ def run_bias_sweep(args):
     print(json.dumps(line))
 
 
+def run_trace_solve(args):
+    """The global FP64 trace solve alone (ddhdg_solve_condensed: nested-
+    dissection multifrontal LU on the device) on the condensed system of the
+    256 x 256 degree-2 diode, timed with CUDA events on the solver's stream.
+    The first call builds the elimination tree, the second captures the
+    numeric sequence in a CUDA graph; both are warm-up."""
+    import torch
+
+    from ddhdg_b200 import _lib
+    from ddhdg_b200 import workloads as cases
+    from ddhdg_b200.solver import NPSolver
+
+    m_side = args.cells_per_side
+    pb, prm, adim = cases.diode(dim=WORKLOAD["dim"], m=m_side, k=WORKLOAD["k"], length=m_side / WORKLOAD["m"])
+    g = NPSolver(pb, prm, adim)
+    g.compute_local_charge_neutrality()
+    for c in (1, 2):
+        _lib.check(g.L.ddhdg_project_density(g._ctx, c, 0.0, g.cell_state.data_ptr(),
+                                             g.trace_state.data_ptr(), g._sp()), "project_density")
+    tt, rhs, fl, dv = g.assemble_condense()
+    n = g.sizes().n_trace_dofs
+    x = torch.zeros(n, dtype=torch.float64, device=g.device)
+
+    def solve():
+        _lib.check(g.L.ddhdg_solve_condensed(g._ctx, tt.data_ptr(), rhs.data_ptr(), fl.data_ptr(), dv.data_ptr(),
+                                             x.data_ptr(), 0, g._sp()), "solve_condensed")
+
+    for _ in range(max(args.warmup, 2)):
+        solve()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(g.stream)
+    for i in range(args.steps):
+        solve()
+        ev[i + 1].record(g.stream)
+    torch.cuda.synchronize()
+    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    line = {"metric": "global trace solve ms (nested-dissection multifrontal LU, FP64)",
+            "value": float(np.mean(per)), "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+            "steps": args.steps, "warmup": max(args.warmup, 2), "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"2D p-n diode {m_side}x{m_side} quads, HDG degree 2, condensed trace system",
+                       "trace_dofs": int(n)},
+            "min_ms": float(np.min(per)), "max_ms": float(np.max(per))}
+    print(json.dumps(line))
+
+
+def run_condense_3d(args):
+    """The condensation of the 3D diode configuration: 64^3 hexahedra (262 144
+    cells), degree 1, step doping along x, ohmic x contacts, SRH, 0.6 V.  The
+    FP64 kernel and the mixed one (FP32 Jacobian, FP64 residuals) on the same
+    state, each timed with CUDA events; the mixed result's largest deviation
+    from the FP64 one is reported relative to the largest FP64 magnitude of
+    each output.  (The full Newton solve of this size is out of reach of the
+    dense nested-dissection fronts: the top separators hold 49 152 dofs.)"""
+    import torch
+
+    from ddhdg_b200 import _lib
+    from ddhdg_b200 import workloads as cases
+    from ddhdg_b200.solver import NPSolver
+
+    m_side = args.cells_per_side if args.cells_per_side != WORKLOAD["m"] else 64
+    out, timing = {}, {}
+    state = None
+    for prec in (0, 1):
+        pb, prm, adim = cases.diode(dim=3, m=m_side, k=1, bias=0.6, precision=prec)
+        g = NPSolver(pb, prm, adim)
+        if state is None:
+            g.compute_local_charge_neutrality()
+            for c in (1, 2):
+                _lib.check(g.L.ddhdg_project_density(g._ctx, c, 0.0, g.cell_state.data_ptr(),
+                                                     g.trace_state.data_ptr(), g._sp()), "project_density")
+            state = (g.get_cell_state(), g.get_trace_state())
+        else:
+            g.set_state(*state)
+        Nt = g.sizes().Nt
+        tt = torch.empty(g.ncells * Nt * Nt, dtype=torch.float64, device=g.device)
+        rhs = torch.empty(g.ncells * Nt, dtype=torch.float64, device=g.device)
+        fl = torch.empty(g.ncells * Nt, dtype=torch.int32, device=g.device)
+        dv = torch.empty(g.ncells * Nt, dtype=torch.float64, device=g.device)
+        torch.cuda.synchronize()
+
+        def condense():
+            _lib.check(g.L.ddhdg_assemble_condense(g._ctx, g.cell_state.data_ptr(), g.trace_state.data_ptr(), 0,
+                                                   tt.data_ptr(), rhs.data_ptr(), fl.data_ptr(), dv.data_ptr(),
+                                                   g._sp()), "condense")
+
+        for _ in range(max(args.warmup, 3)):
+            condense()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        steps = min(args.steps, 20)
+        e0.record(g.stream)
+        for _ in range(steps):
+            condense()
+        e1.record(g.stream)
+        torch.cuda.synchronize()
+        timing[prec] = e0.elapsed_time(e1) / steps
+        out[prec] = (tt, rhs)
+        ncells = g.ncells
+        del g, fl, dv
+        torch.cuda.empty_cache()
+    (t64, r64), (t32, r32) = out[0], out[1]
+    e_tt = float((t32 - t64).abs().max() / t64.abs().max())
+    e_rhs = float((r32 - r64).abs().max() / r64.abs().max())
+    line = {"metric": "HDG cells condensed/s, 3D diode (FP64 and mixed precision)",
+            "value": ncells / (timing[1] * 1e-3), "unit": "cells/s", "higher_is_better": True, "n_gpus": 1,
+            "dtype": "f32 Jacobian / f64 residual", "data": "synthetic",
+            "config": {"workload": f"3D p-n diode {m_side}^3 hexahedra, HDG degree 1, 0.6 V, SRH",
+                       "cells": ncells},
+            "condense_ms": {"fp64": timing[0], "mixed": timing[1]},
+            "cells_per_s": {"fp64": ncells / (timing[0] * 1e-3), "mixed": ncells / (timing[1] * 1e-3)},
+            "mixed_vs_fp64_rel_diff": {"tt": e_tt, "rhs": e_rhs}}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -304,6 +419,10 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=4.0, help="arrivals per second")
     ap.add_argument("--bias-sweep", action="store_true",
                     help="time the warm-started 0..0.8 V sweep (17 points) instead of the step")
+    ap.add_argument("--trace-solve", action="store_true",
+                    help="time the global trace solve alone (nested dissection) on the diode's condensed system")
+    ap.add_argument("--condense-3d", action="store_true",
+                    help="condensation of the 3D 64^3 degree-1 diode at 0.6 V, FP64 and mixed")
     ap.add_argument("--cells-per-side", type=int, default=WORKLOAD["m"],
                     help="smaller meshes of the same diode for profiling runs")
     args = ap.parse_args()
@@ -313,6 +432,10 @@ def main():
         return run_bias_sweep(args)
     if args.serve:
         return run_serve(args)
+    if args.trace_solve:
+        return run_trace_solve(args)
+    if args.condense_3d:
+        return run_condense_3d(args)
 
     import torch
     import torch.distributed as dist
@@ -480,7 +603,7 @@ def main():
     prm.consistent_recombination_jacobian = True
     gn = NPSolver(pb, prm, adim, device=str(dev))
     gn.set_state(g.get_cell_state(), g.get_trace_state())
-    gn.private_run(0.0, 0.0, 1)  # builds the elimination tree (host plan + fronts)
+    gn.private_run(0.0, 0.0, 2)  # builds the elimination tree, then captures the solve graph
     torch.cuda.synchronize()
     newton_steps = 3
     gn.set_state(g.get_cell_state(), g.get_trace_state())
