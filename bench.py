@@ -531,12 +531,14 @@ def main():
     d2h = pin_out.numel() * 8
 
     def e2e_step():
-        g.cell_state.copy_(pin_cell, non_blocking=True)
-        g.trace_state.copy_(pin_trace, non_blocking=True)
-        dtrace.copy_(pin_dtrace, non_blocking=True)
-        condense()
-        reconstruct()
-        pin_out.copy_(dcell, non_blocking=True)
+        # the host-buffer entry points: the state is read from and the cell
+        # update written to pinned host memory by the calls themselves, the
+        # copies overlapping the kernels chunk by chunk
+        _lib.check(L.ddhdg_assemble_condense_host(g._ctx, pin_cell.data_ptr(), pin_trace.data_ptr(), 0,
+                                                  tt.data_ptr(), rhs.data_ptr(), dflag.data_ptr(),
+                                                  dval.data_ptr(), sp), "condense (host buffers)")
+        _lib.check(L.ddhdg_reconstruct_host(g._ctx, pin_dtrace.data_ptr(), 0, pin_out.data_ptr(), sp),
+                   "reconstruct (host buffers)")
 
     for _ in range(2):
         e2e_step()

@@ -142,6 +142,37 @@ struct ddhdg_ctx
   int                t_steps    = 0;
   DevBuf<double>     norm_buf;
   DevBuf<int64_t>    d_face_cells, d_face_local;
+  // host-buffer calls: device copies of the state and of the reconstruction
+  // input and output, a copy stream per direction, events per chunk
+  struct HostIO
+  {
+    static constexpr int NChunk = 4;
+    DevBuf<double>       cell, trace, dtrace, dcell;
+    cudaStream_t         h2d = nullptr, d2h = nullptr;
+    cudaEvent_t          ev_trace = nullptr, ev_out = nullptr;
+    // recorded after the last kernel that reads the device state copies /
+    // the trace-update copy: the next upload into them waits for it only
+    cudaEvent_t          ev_cell_free = nullptr, ev_dtrace_free = nullptr;
+    cudaEvent_t          ev_chunk[NChunk] = {}, ev_rec[NChunk] = {};
+    bool                 ready = false, have_state = false;
+    ~HostIO()
+    {
+      for (cudaEvent_t e : {ev_trace, ev_out, ev_cell_free, ev_dtrace_free})
+        if (e)
+          cudaEventDestroy(e);
+      for (int k = 0; k < NChunk; ++k)
+        {
+          if (ev_chunk[k])
+            cudaEventDestroy(ev_chunk[k]);
+          if (ev_rec[k])
+            cudaEventDestroy(ev_rec[k]);
+        }
+      if (h2d)
+        cudaStreamDestroy(h2d);
+      if (d2h)
+        cudaStreamDestroy(d2h);
+    }
+  } hio;
 };
 
 namespace
@@ -1151,11 +1182,11 @@ ddhdg_set_enabled(ddhdg_ctx *c, int V, int n, int p)
   return DDHDG_OK;
 }
 
-int
-ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
-                        const double *trace_state, int thermo, double *tt,
-                        double *rhs, int32_t *dflag, double *dval,
-                        ddhdg_stream_t stream)
+// the condense launch over the cells [c0, c1)
+static int
+condense_range(ddhdg_ctx *c, const double *cell_state, const double *trace_state, int thermo,
+               double *tt, double *rhs, int32_t *dflag, double *dval, ddhdg_stream_t stream,
+               int64_t c0, int64_t c1)
 {
   if (!c || !cell_state || !trace_state || !tt || !rhs || !dflag || !dval)
     return fail(DDHDG_BAD_ARG, "null argument");
@@ -1170,6 +1201,8 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
   if (!kernels_for(c->dim, c->k, cf, rf, mixed))
     return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
   KParams P     = make_params(c, thermo);
+  P.cell0       = c0;
+  P.ncells      = c1;
   P.cell_state  = cell_state;
   P.trace_state = trace_state;
   P.tt          = tt;
@@ -1193,7 +1226,7 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
       P.stage = 0;
       threads = wpb * 32;
       smem    = (size_t)wpb * per;
-      units   = (c->ncells + wpb - 1) / wpb;
+      units   = (c1 - c0 + wpb - 1) / wpb;
     }
   else
     {
@@ -1205,7 +1238,7 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
       P.chunk = chunk;
       P.stage = stage;
       threads = CondenseTPB;
-      units   = c->ncells;
+      units   = c1 - c0;
       if (r_global)
         {
           int per_sm = 0;
@@ -1222,10 +1255,21 @@ ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, threads, smem));
   if (per_sm < 1)
     return fail(DDHDG_BAD_ARG, "condense kernel does not fit on an SM");
-  const int grid = (int)std::min<int64_t>(units, (int64_t)per_sm * c->sm_count);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(units, (int64_t)per_sm * c->sm_count));
   cf.launch(c->T, P, grid, threads, smem, (cudaStream_t)stream);
   CK(cudaGetLastError());
   return DDHDG_OK;
+}
+
+int
+ddhdg_assemble_condense(ddhdg_ctx *c, const double *cell_state,
+                        const double *trace_state, int thermo, double *tt,
+                        double *rhs, int32_t *dflag, double *dval,
+                        ddhdg_stream_t stream)
+{
+  if (!c)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  return condense_range(c, cell_state, trace_state, thermo, tt, rhs, dflag, dval, stream, 0, c->ncells);
 }
 
 int
@@ -1248,10 +1292,11 @@ ddhdg_solve_condensed(ddhdg_ctx *c, const double *tt, const double *rhs, const i
   return DDHDG_OK;
 }
 
-int
-ddhdg_reconstruct(ddhdg_ctx *c, const double *cell_state, const double *trace_state,
+// the reconstruction launch over the cells [c0, c1)
+static int
+reconstruct_range(ddhdg_ctx *c, const double *cell_state, const double *trace_state,
                   const double *update_trace, double *update_cell, int thermo,
-                  ddhdg_stream_t stream)
+                  ddhdg_stream_t stream, int64_t c0, int64_t c1)
 {
   if (!c || !cell_state || !trace_state || !update_trace || !update_cell)
     return fail(DDHDG_BAD_ARG, "null argument");
@@ -1264,6 +1309,8 @@ ddhdg_reconstruct(ddhdg_ctx *c, const double *cell_state, const double *trace_st
   if (!kernels_for(c->dim, c->k, cf, rf))
     return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
   KParams P     = make_params(c, thermo);
+  P.cell0       = c0;
+  P.ncells      = c1;
   P.cell_state  = cell_state;
   P.trace_state = trace_state;
   P.ycache      = m.ycache.p;
@@ -1277,11 +1324,131 @@ ddhdg_reconstruct(ddhdg_ctx *c, const double *cell_state, const double *trace_st
   CK(allow_full_dynamic_smem(reinterpret_cast<const void *>(rf)));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rf, wpb * 32, smem));
-  const int64_t blocks_needed = (c->ncells + wpb - 1) / wpb;
+  const int64_t blocks_needed = (c1 - c0 + wpb - 1) / wpb;
   const int     grid =
     (int)std::max<int64_t>(1, std::min<int64_t>(blocks_needed, (int64_t)std::max(per_sm, 1) * c->sm_count));
   rf<<<grid, wpb * 32, smem, (cudaStream_t)stream>>>(P, update_trace, update_cell);
   CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+int
+ddhdg_reconstruct(ddhdg_ctx *c, const double *cell_state, const double *trace_state,
+                  const double *update_trace, double *update_cell, int thermo,
+                  ddhdg_stream_t stream)
+{
+  if (!c)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  return reconstruct_range(c, cell_state, trace_state, update_trace, update_cell, thermo, stream, 0,
+                           c->ncells);
+}
+
+// device copies, copy streams and events of the host-buffer calls (first use)
+static int
+hostio_setup(ddhdg_ctx *c)
+{
+  auto &h = c->hio;
+  if (h.ready)
+    return DDHDG_OK;
+  const size_t ncell = (size_t)c->ncells * 3 * (c->dim + 1) * c->nb;
+  const size_t ntr   = (size_t)c->nfaces * 3 * c->nf;
+  int          r;
+  if ((r = h.cell.alloc(ncell)) || (r = h.trace.alloc(ntr)) || (r = h.dtrace.alloc(ntr)) ||
+      (r = h.dcell.alloc(ncell)))
+    return r;
+  CK(cudaStreamCreateWithFlags(&h.h2d, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h.d2h, cudaStreamNonBlocking));
+  for (cudaEvent_t *e : {&h.ev_trace, &h.ev_out, &h.ev_cell_free, &h.ev_dtrace_free})
+    CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  for (int k = 0; k < ddhdg_ctx::HostIO::NChunk; ++k)
+    {
+      CK(cudaEventCreateWithFlags(&h.ev_chunk[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&h.ev_rec[k], cudaEventDisableTiming));
+    }
+  h.ready = true;
+  return DDHDG_OK;
+}
+
+static int64_t
+hostio_chunk_begin(const ddhdg_ctx *c, int k)
+{
+  return c->ncells * k / ddhdg_ctx::HostIO::NChunk;
+}
+
+int
+ddhdg_assemble_condense_host(ddhdg_ctx *c, const double *cell_state_host,
+                             const double *trace_state_host, int thermo, double *tt, double *rhs,
+                             int32_t *dflag, double *dval, ddhdg_stream_t stream)
+{
+  if (!c || !cell_state_host || !trace_state_host || !tt || !rhs || !dflag || !dval)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  int r;
+  if ((r = hostio_setup(c)))
+    return r;
+  auto        &h  = c->hio;
+  cudaStream_t s  = (cudaStream_t)stream;
+  const size_t pc = (size_t)3 * (c->dim + 1) * c->nb; // doubles per cell
+  // the device copies are rewritten once the kernels that read them (the
+  // previous condensation or reconstruction) are done
+  CK(cudaStreamWaitEvent(h.h2d, h.ev_cell_free, 0));
+  CK(cudaMemcpyAsync(h.trace.p, trace_state_host, (size_t)c->nfaces * 3 * c->nf * sizeof(double),
+                     cudaMemcpyHostToDevice, h.h2d));
+  CK(cudaEventRecord(h.ev_trace, h.h2d));
+  for (int k = 0; k < ddhdg_ctx::HostIO::NChunk; ++k)
+    {
+      const int64_t c0 = hostio_chunk_begin(c, k), c1 = hostio_chunk_begin(c, k + 1);
+      CK(cudaMemcpyAsync(h.cell.p + c0 * pc, cell_state_host + c0 * pc, (size_t)(c1 - c0) * pc * sizeof(double),
+                         cudaMemcpyHostToDevice, h.h2d));
+      CK(cudaEventRecord(h.ev_chunk[k], h.h2d));
+    }
+  CK(cudaStreamWaitEvent(s, h.ev_trace, 0));
+  for (int k = 0; k < ddhdg_ctx::HostIO::NChunk; ++k)
+    {
+      const int64_t c0 = hostio_chunk_begin(c, k), c1 = hostio_chunk_begin(c, k + 1);
+      CK(cudaStreamWaitEvent(s, h.ev_chunk[k], 0));
+      if (c1 > c0 &&
+          (r = condense_range(c, h.cell.p, h.trace.p, thermo, tt, rhs, dflag, dval, stream, c0, c1)))
+        return r;
+    }
+  CK(cudaEventRecord(h.ev_cell_free, s));
+  h.have_state = true;
+  return DDHDG_OK;
+}
+
+int
+ddhdg_reconstruct_host(ddhdg_ctx *c, const double *update_trace_host, int thermo,
+                       double *update_cell_host, ddhdg_stream_t stream)
+{
+  if (!c || !update_trace_host || !update_cell_host)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  auto &h = c->hio;
+  if (!h.have_state)
+    return fail(DDHDG_BAD_ARG, "ddhdg_reconstruct_host needs a preceding ddhdg_assemble_condense_host");
+  cudaStream_t s  = (cudaStream_t)stream;
+  const size_t pc = (size_t)3 * (c->dim + 1) * c->nb;
+  int          r;
+  // the upload of the trace update may overlap the condensation still running
+  CK(cudaStreamWaitEvent(h.h2d, h.ev_dtrace_free, 0));
+  CK(cudaMemcpyAsync(h.dtrace.p, update_trace_host, (size_t)c->nfaces * 3 * c->nf * sizeof(double),
+                     cudaMemcpyHostToDevice, h.h2d));
+  CK(cudaEventRecord(h.ev_trace, h.h2d));
+  CK(cudaStreamWaitEvent(s, h.ev_trace, 0));
+  for (int k = 0; k < ddhdg_ctx::HostIO::NChunk; ++k)
+    {
+      const int64_t c0 = hostio_chunk_begin(c, k), c1 = hostio_chunk_begin(c, k + 1);
+      if (c1 <= c0)
+        continue;
+      if ((r = reconstruct_range(c, h.cell.p, h.trace.p, h.dtrace.p, h.dcell.p, thermo, stream, c0, c1)))
+        return r;
+      CK(cudaEventRecord(h.ev_rec[k], s));
+      CK(cudaStreamWaitEvent(h.d2h, h.ev_rec[k], 0));
+      CK(cudaMemcpyAsync(update_cell_host + c0 * pc, h.dcell.p + c0 * pc, (size_t)(c1 - c0) * pc * sizeof(double),
+                         cudaMemcpyDeviceToHost, h.d2h));
+    }
+  CK(cudaEventRecord(h.ev_cell_free, s));
+  CK(cudaEventRecord(h.ev_dtrace_free, s));
+  CK(cudaEventRecord(h.ev_out, h.d2h));
+  CK(cudaStreamWaitEvent(s, h.ev_out, 0));
   return DDHDG_OK;
 }
 

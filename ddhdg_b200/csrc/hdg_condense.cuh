@@ -172,7 +172,7 @@ namespace ddhdg
       ce_of[P.comps[c]] = c;
     const bool nen = ce_of[1] >= 0, pen = ce_of[2] >= 0;
 
-    for (int64_t cell = blockIdx.x; cell < P.ncells; cell += gridDim.x)
+    for (int64_t cell = P.cell0 + blockIdx.x; cell < P.ncells; cell += gridDim.x)
       {
         // ------------------------------------------------------ state
         const double *cs = P.cell_state + cell * NCA;

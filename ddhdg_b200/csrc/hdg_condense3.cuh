@@ -1,4 +1,5 @@
-// Per-cell assembly + static condensation, one warp per cell (sm_100a, FP64),
+// Per-cell assembly + static condensation, one warp per cell (sm_100a, FP64
+// or with an FP32 Jacobian),
 // for local scalar systems of at most 32 unknowns (3 (k+1)^d <= 32: 2D k <= 2,
 // 3D k = 1, 1D).
 //
@@ -183,8 +184,11 @@ namespace ddhdg
     *reinterpret_cast<float2 *>(p) = make_float2(a, b);
   }
 
-  // JT: the Jacobian type (double: the FP64 kernel; float: the mixed kernel,
-  // see the note on precision below)
+  // JT: the Jacobian type.  double: the FP64 kernel.  float: the mixed
+  // kernel, where the linearised operators, S and its inverse, R / Y, T and
+  // the trace-row weights are FP32 and the products accumulate in FP64 on the
+  // tensor path, while the state, every residual and the outputs stay FP64
+  // (a Newton loop on these blocks converges to the FP64 solution).
   template <int DIM, int K, typename JT = double>
   __global__ void __launch_bounds__(Condense3MaxWPB * 32, sizeof(JT) == 8 ? 1 : 2)
   condense3_kernel(const KParams P, const __grid_constant__ CTab<DIM, K> C)
@@ -261,7 +265,7 @@ namespace ddhdg
       }
     const int wpb = blockDim.x >> 5;
 
-    for (int64_t cell = (int64_t)blockIdx.x * wpb + warp; cell < P.ncells;
+    for (int64_t cell = P.cell0 + (int64_t)blockIdx.x * wpb + warp; cell < P.ncells;
          cell += (int64_t)gridDim.x * wpb)
       {
         // keeps the table loads inside the cell loop (no hoisting of

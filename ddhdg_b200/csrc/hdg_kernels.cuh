@@ -23,7 +23,8 @@ namespace ddhdg
   {
     // mesh
     int     n[3];
-    int64_t ncells;
+    int64_t ncells; // cells [cell0, ncells) are processed by a launch
+    int64_t cell0;
     int64_t face_off[3];
     int     face_ext[3][3];
     // tables (device, global) and their layout
@@ -119,7 +120,7 @@ namespace ddhdg
     double *unew = lnew + F * 3 * nf;
     double *dlr  = unew + nb;        // [Nt] trace update, restricted order
 
-    for (int64_t cell = (int64_t)blockIdx.x * P.wpb + warp; cell < P.ncells;
+    for (int64_t cell = P.cell0 + (int64_t)blockIdx.x * P.wpb + warp; cell < P.ncells;
          cell += (int64_t)gridDim.x * P.wpb)
       {
         for (int i = lane; i < F * 3 * nf; i += 32)

@@ -213,6 +213,28 @@ int ddhdg_reconstruct(ddhdg_ctx *ctx, const double *cell_state,
                       double *update_cell, int thermo_eq,
                       ddhdg_stream_t stream);
 
+/* The same two calls for callers whose state lives in host memory, as the
+ * reference's NPSolver keeps current_solution_cell / current_solution_trace
+ * and update_cell in host vectors (include/np_solver.h:881-887): the host
+ * arrays are read and written by the calls themselves, and the copies overlap
+ * the kernels.  ddhdg_assemble_condense_host copies the trace state, then the
+ * cell state in 4 chunks of cells on an internal copy stream; each chunk is
+ * condensed on `stream` as soon as it has arrived.  The context keeps the
+ * device copies of the state.  ddhdg_reconstruct_host reconstructs that state
+ * for update_trace in the same chunks and copies each chunk of update_cell
+ * back on a second copy stream while the next chunk runs; the results are in
+ * host memory when `stream` has completed.  Outputs of the condensation (tt,
+ * rhs, dflag, dval) are device arrays as in ddhdg_assemble_condense.  The copies
+ * overlap only for page-locked host memory (cudaHostAlloc / cudaHostRegister);
+ * pageable memory gives the same results with serialised copies.  A context's
+ * host-buffer calls must be issued on one stream at a time. */
+int ddhdg_assemble_condense_host(ddhdg_ctx *ctx, const double *cell_state_host,
+                                 const double *trace_state_host, int thermo_eq, double *tt,
+                                 double *rhs, int32_t *dflag, double *dval,
+                                 ddhdg_stream_t stream);
+int ddhdg_reconstruct_host(ddhdg_ctx *ctx, const double *update_trace_host, int thermo_eq,
+                           double *update_cell_host, ddhdg_stream_t stream);
+
 /* private_run (src/np_solver.cpp:1452-1561) on device-resident state:
  * Newton iterations with damping alpha, absolute / relative stop on the
  * infinity norm of the update.  cell_state / trace_state are updated in
