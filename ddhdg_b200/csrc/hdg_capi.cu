@@ -138,6 +138,7 @@ struct ddhdg_ctx
   cusparseMatDescr_t descr    = nullptr;
   // face -> adjacent cells
   std::vector<int64_t> face_cells; // [nfaces][2] (-1 when absent)
+  bool               solver_graphs = true; // CUDA-graph capture of the trace solve
   double             t_condense = 0., t_solve = 0., t_recon = 0.;
   int                t_steps    = 0;
   DevBuf<double>     norm_buf;
@@ -931,6 +932,7 @@ namespace
         const int                 r = nd->build(M, err);
         if (r)
           return fail(r, err);
+        nd->set_graphs(c->solver_graphs);
         m.nd = std::move(nd);
       }
     out = m.nd.get();
@@ -1289,6 +1291,18 @@ ddhdg_solve_condensed(ddhdg_ctx *c, const double *tt, const double *rhs, const i
   std::string err;
   if ((r = nd->solve(tt, rhs, dflag, dval, m.Nt, x, (cudaStream_t)stream, c->sm_count, err)))
     return fail(r, err);
+  return DDHDG_OK;
+}
+
+int
+ddhdg_set_solver_graphs(ddhdg_ctx *c, int enable)
+{
+  if (!c)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  c->solver_graphs = enable != 0;
+  for (auto &m : c->mode)
+    if (m.nd)
+      m.nd->set_graphs(c->solver_graphs);
   return DDHDG_OK;
 }
 

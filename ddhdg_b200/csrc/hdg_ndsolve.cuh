@@ -902,6 +902,18 @@ namespace ddhdg
     // blocks.  The whole sequence (about 10 launches per batch) is captured
     // in a CUDA graph on the second call with the same buffers and replayed
     // after that; the check for singular fronts stays outside the graph.
+    // capture and replay of the numeric sequence on (default) or off
+    void
+    set_graphs(bool on)
+    {
+      use_graphs_ = on;
+      if (!on && exec_)
+        {
+          cudaGraphExecDestroy(exec_);
+          exec_ = nullptr;
+        }
+    }
+
     int
     solve(const double *tt, const double *rhs, const int32_t *dflag, const double *dval, int Nt,
           double *x, cudaStream_t s, int sm_count, std::string &err)
@@ -912,12 +924,12 @@ namespace ddhdg
         return bad(err, "trace block size does not match the solver");
       const Key k{tt, rhs, dflag, dval, x, sm_count};
       int       r = DDHDG_OK;
-      if (graphs_ok_ && exec_ && k == key_)
+      if (use_graphs_ && graphs_ok_ && exec_ && k == key_)
         {
           if (cudaGraphLaunch(exec_, s) != cudaSuccess)
             return bad(err, "cudaGraphLaunch failed", DDHDG_CUDA_ERROR);
         }
-      else if (graphs_ok_ && k == key_ && !exec_)
+      else if (use_graphs_ && graphs_ok_ && k == key_ && !exec_)
         {
           // same buffers as the last (eager) call: capture, then launch
           cudaGraph_t gph = nullptr;
@@ -1413,6 +1425,7 @@ namespace ddhdg
     cudaStream_t        cap_              = nullptr; // stream the graph is captured on
     cudaGraphExec_t     exec_             = nullptr;
     Key                 key_{};
-    bool                graphs_ok_ = true;
+    bool                graphs_ok_ = true;  // capture works in this build
+    bool                use_graphs_ = true; // the caller wants graphs
   };
 } // namespace ddhdg

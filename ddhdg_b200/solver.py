@@ -370,6 +370,12 @@ class NPSolver:
         xs = x.cpu().numpy()
         return {c: xs[d] for c, d in self._component_dofs(sysm["thermo"]).items()}
 
+    def set_solver_graphs(self, enable: bool):
+        """Capture the trace solve's launch sequence in a CUDA graph on the
+        second solve with the same buffers and replay it afterwards (on by
+        default); off: every solve launches its kernels directly."""
+        _lib.check(self.L.ddhdg_set_solver_graphs(self._ctx, int(bool(enable))), "set_solver_graphs")
+
     def private_run(self, abs_tol, rel_tol, max_it, thermo=False, alpha=None):
         alpha = self.parameters.nonlinear_parameters.alpha if alpha is None else alpha
         it = ctypes.c_int()

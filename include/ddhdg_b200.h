@@ -204,6 +204,15 @@ int ddhdg_solve_condensed(ddhdg_ctx *ctx, const double *tt, const double *rhs,
                           const int32_t *dflag, const double *dval, double *x,
                           int thermo_eq, ddhdg_stream_t stream);
 
+/* No counterpart in the reference (its solve is UMFPACK or GMRES on the
+ * host).  Whether ddhdg_solve_condensed (and so ddhdg_newton) captures the
+ * numeric sequence of the trace solve in a CUDA graph on its second call with
+ * the same buffers and replays it afterwards: enable = 1, the default.  With
+ * enable = 0 every solve launches its kernels directly: no capture or
+ * instantiation cost, for callers whose buffers change from call to call or
+ * that make only a couple of solves per context.  Both give the same bits. */
+int ddhdg_set_solver_graphs(ddhdg_ctx *ctx, int enable);
+
 /* assemble_system(true, thermo_eq): cell update from the full trace update
  * update_trace [nfaces][3][nf] (include/assembling_methods.template.h:
  * 2122-2160 and 2688-2697).  Uses the reconstruction data kept by the last

@@ -53,7 +53,11 @@ def _csr(torch, g, tt, rhs, fl, dv):
     return A, grhs.cpu().numpy()
 
 
-@pytest.mark.parametrize("dim,m,k", [(1, 16, 2), (2, 16, 1), (2, 8, 2), (2, 9, 2), (3, 3, 1), (3, 2, 2)])
+# 48 x 48 at degree 2: the root separator has 432 eliminated dofs, so the top
+# fronts take the per-front dense LU path; the smaller meshes cover the fused
+# small-front kernel, the one-CTA mid-front kernel and batched cuBLAS
+@pytest.mark.parametrize("dim,m,k", [(1, 16, 2), (2, 16, 1), (2, 8, 2), (2, 9, 2), (3, 3, 1), (3, 2, 2),
+                                     (2, 48, 2)])
 def test_nested_dissection_matches_sparse_lu(dim, m, k):
     import scipy.sparse.linalg as spla
 
@@ -62,7 +66,9 @@ def test_nested_dissection_matches_sparse_lu(dim, m, k):
     A, b = _csr(torch, g, tt, rhs, fl, dv)
     x_lu = spla.splu(A.tocsc()).solve(b)
     x = torch.full((A.shape[0],), float("nan"), dtype=torch.float64, device=g.device)
-    for _ in range(2):  # the second call reuses the elimination tree
+    # the second call reuses the elimination tree and captures the numeric
+    # sequence in a CUDA graph, the third replays it
+    for _ in range(3):
         _lib.check(g.L.ddhdg_solve_condensed(g._ctx, tt.data_ptr(), rhs.data_ptr(), fl.data_ptr(),
                                              dv.data_ptr(), x.data_ptr(), 0, g._sp()), "solve_condensed")
         torch.cuda.synchronize()
@@ -74,3 +80,33 @@ def test_nested_dissection_matches_sparse_lu(dim, m, k):
         r_nd = np.abs(A @ xg - b).max()
         r_lu = np.abs(A @ x_lu - b).max()
         assert r_nd <= 100 * r_lu + 1e-12 * np.abs(b).max()
+
+
+def test_solver_graphs_switch_gives_the_same_solution():
+    """ddhdg_set_solver_graphs: eager launches and the captured graph run the
+    same kernels on the same data, so the solutions are bitwise equal; the
+    switch can be flipped between solves (turning it off drops the graph)."""
+    torch, g = _setup(2, 16, 2)
+    tt, rhs, fl, dv = g.assemble_condense()
+    n = g.sizes().n_trace_dofs
+    sols = {}
+    for graphs in (True, False, True):
+        g.set_solver_graphs(graphs)
+        for rep in range(3):
+            x = torch.full((n,), float("nan"), dtype=torch.float64, device=g.device)
+            # fresh output buffers every call, then the same buffer three times
+            _lib.check(g.L.ddhdg_solve_condensed(g._ctx, tt.data_ptr(), rhs.data_ptr(), fl.data_ptr(),
+                                                 dv.data_ptr(), x.data_ptr(), 0, g._sp()), "solve_condensed")
+            torch.cuda.synchronize()
+            sols.setdefault(graphs, []).append(x.cpu().numpy())
+        xs = torch.full((n,), float("nan"), dtype=torch.float64, device=g.device)
+        for rep in range(3):
+            _lib.check(g.L.ddhdg_solve_condensed(g._ctx, tt.data_ptr(), rhs.data_ptr(), fl.data_ptr(),
+                                                 dv.data_ptr(), xs.data_ptr(), 0, g._sp()), "solve_condensed")
+            torch.cuda.synchronize()
+            sols[graphs].append(xs.cpu().numpy())
+    ref = sols[True][0]
+    assert np.isfinite(ref).all()
+    for graphs, xs_ in sols.items():
+        for x in xs_:
+            assert np.array_equal(x, ref), graphs
