@@ -991,9 +991,17 @@ ddhdg_ctx_create(const ddhdg_problem_desc *d, ddhdg_ctx **out)
     if (d->precision == 1 && 3 * nb > 32)
       return fail(DDHDG_BAD_ARG, "mixed precision needs 3 (k+1)^d <= 32 (1D, 2D k <= 2, 3D k = 1)");
   }
-  for (int a = 0; a < d->dim; ++a)
-    if (d->n[a] < 1 || !(d->h[a] > 0.))
-      return fail(DDHDG_BAD_ARG, "bad mesh");
+  {
+    int64_t cells = 1;
+    for (int a = 0; a < d->dim; ++a)
+      {
+        if (d->n[a] < 1 || !(d->h[a] > 0.))
+          return fail(DDHDG_BAD_ARG, "bad mesh");
+        cells *= d->n[a];
+        if (cells >= (int64_t(1) << 31))
+          return fail(DDHDG_BAD_ARG, "a context holds fewer than 2^31 cells");
+      }
+  }
   if (!d->doping_host || !d->face_bc_host || !d->face_bc_val_host)
     return fail(DDHDG_BAD_ARG, "doping and boundary tables are required");
   int ndev = 0;

@@ -70,10 +70,14 @@ namespace ddhdg
   __device__ inline int64_t
   face_index(const KParams &P, int64_t cell, int f, int dim)
   {
-    int ci[3];
-    ci[0]       = (int)(cell % P.n[0]);
-    ci[1]       = (int)((cell / P.n[0]) % P.n[1]);
-    ci[2]       = (int)(cell / ((int64_t)P.n[0] * P.n[1]));
+    // 32-bit divisions: contexts hold fewer than 2^31 cells
+    int            ci[3];
+    const unsigned c  = (unsigned)cell;
+    const unsigned n0 = (unsigned)P.n[0], n1 = (unsigned)P.n[1];
+    const unsigned q  = c / n0;
+    ci[0]             = (int)(c - q * n0);
+    ci[1]             = (int)(q % n1);
+    ci[2]             = (int)(q / n1);
     const int a = f / 2;
     ci[a] += f % 2;
     int64_t idx = 0, stride = 1;
@@ -90,7 +94,7 @@ namespace ddhdg
   // unknowns, and the flux unknowns from the (linear) flux rows,
   // W_new = P u_new - Q lam_new, i.e. dW = P(u0+du) - W0 - Q(lam0+dlam).
   template <int DIM, int K>
-  __global__ void __launch_bounds__(256)
+  __global__ void __launch_bounds__(256, 8) // 8 CTAs per SM: memory-latency bound
   reconstruct_kernel(const KParams P, const double *__restrict__ dtrace,
                      double *__restrict__ dcell)
   {
@@ -123,13 +127,20 @@ namespace ddhdg
     for (int64_t cell = P.cell0 + (int64_t)blockIdx.x * P.wpb + warp; cell < P.ncells;
          cell += (int64_t)gridDim.x * P.wpb)
       {
-        for (int i = lane; i < F * 3 * nf; i += 32)
+        // the cell's face ids: one lane per face, then shuffled (the loop
+        // runs the same number of times on every lane)
+        const int64_t my_face = face_index(P, cell, lane < F ? lane : 0, DIM);
+        for (int i0 = 0; i0 < F * 3 * nf; i0 += 32)
           {
-            const int     f  = i / (3 * nf);
-            const int64_t Fi = face_index(P, cell, f, DIM);
-            const double  d  = dtrace[Fi * 3 * nf + (i % (3 * nf))];
-            dl[i]            = d;
-            lnew[i]          = P.trace_state[Fi * 3 * nf + (i % (3 * nf))] + d;
+            const int     i  = i0 + lane;
+            const bool    in = i < F * 3 * nf;
+            const int64_t Fi = __shfl_sync(0xffffffffu, my_face, in ? i / (3 * nf) : 0);
+            if (in)
+              {
+                const double d = dtrace[Fi * 3 * nf + (i % (3 * nf))];
+                dl[i]          = d;
+                lnew[i]        = P.trace_state[Fi * 3 * nf + (i % (3 * nf))] + d;
+              }
           }
         __syncwarp();
         for (int t = lane; t < Nt; t += 32)
