@@ -82,15 +82,15 @@ def _start(pb, prm, adim):
     return o
 
 
-@pytest.mark.parametrize("k,m,bias", [(1, 32, 0.0), (2, 32, 0.3)])
-def test_mixed_newton_matches_fp64(k, m, bias):
+@pytest.mark.parametrize("dim,k,m,bias", [(2, 1, 32, 0.0), (2, 2, 32, 0.3), (3, 1, 8, 0.2)])
+def test_mixed_newton_matches_fp64(dim, k, m, bias):
     """Newton from the equilibrium state, FP64 and mixed, same start: both
     converge and the final fields agree to 1e-8 relative.  The mixed loop may
     take a few more iterations (linear instead of quadratic end phase)."""
     NPSolver = _npsolver()
     res, states = {}, {}
     for prec in (Precision.fp64, Precision.mixed):
-        pb, prm, adim = cases.diode(dim=2, m=m, k=k, bias=bias, precision=prec)
+        pb, prm, adim = cases.diode(dim=dim, m=m, k=k, bias=bias, precision=prec)
         prm.consistent_drift_jacobian = True
         prm.consistent_recombination_jacobian = True
         o = _start(pb, prm, adim)
@@ -100,9 +100,9 @@ def test_mixed_newton_matches_fp64(k, m, bias):
         states[prec] = (g.get_cell_state(), g.get_trace_state())
     r64, r32 = res[Precision.fp64], res[Precision.mixed]
     assert r64.converged and r32.converged
-    print(f"k={k} m={m} bias={bias}: FP64 {r64.iterations} iterations, mixed {r32.iterations}")
+    print(f"{dim}D k={k} m={m} bias={bias}: FP64 {r64.iterations} iterations, mixed {r32.iterations}")
     assert r32.iterations <= r64.iterations + 6
     (c64, t64), (c32, t32) = states[Precision.fp64], states[Precision.mixed]
-    e = _field_rel_err(c32, c64, t32, t64, 2, (k + 1) ** 2)
+    e = _field_rel_err(c32, c64, t32, t64, dim, (k + 1) ** dim)
     print(f"  final field error of mixed against FP64: {e:.2e}")
     assert e < FINAL_TOL, e
