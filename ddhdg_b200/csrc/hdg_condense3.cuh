@@ -132,10 +132,14 @@ namespace ddhdg
     o.rf   = take(3 * Fq);
     const int dead_end = p;
     p     = 0;
+    // 3D FP64: the per-row face weights times coefficients (rA, rS, rD) are
+    // recomputed where they are used (shared memory sets the warps per SM;
+    // the mixed kernel is issue-bound and keeps them)
+    const bool rw = dim == 3 && jb == 8;
     o.Trs = take_j(Ns * Nt);
-    o.rA  = take_j(Nt * 3 * nqf);
-    o.rS  = take_j(Nt * nqf);
-    o.rD  = take_j(Nt * nqf);
+    o.rA  = take_j(rw ? 0 : Nt * 3 * nqf);
+    o.rS  = take_j(rw ? 0 : Nt * nqf);
+    o.rD  = take_j(rw ? 0 : Nt * nqf);
     o.rZ  = take(Nt);
     o.H   = take(3 * Fq);
     p     = p > dead_end ? p : dead_end;
@@ -203,6 +207,7 @@ namespace ddhdg
     constexpr int Ft    = F * nf;
     constexpr int NCA   = Dm::Nc_all;
     constexpr int NSMAX = 3 * nb;
+    constexpr bool RW   = DIM == 3 && sizeof(JT) == 8; // recompute rA / rS / rD (see ws3_layout)
     static_assert(NSMAX <= 32, "one lane per row of the scalar system");
     extern __shared__ __align__(16) double smem[];
     __shared__ int piv3[Condense3MaxWPB][NSMAX];
@@ -997,13 +1002,17 @@ namespace ddhdg
               {
                 const int    fq = fi * nqf + qf;
                 const double w  = w_f[fq] * xi[qf * nf + mi];
-                rS[i * nqf + qf] = w * tcS[b * Fq + fq];
-                rD[i * nqf + qf] = w * ttc[b * Fq + fq];
+                if (!RW)
+                  {
+                    rS[i * nqf + qf] = w * tcS[b * Fq + fq];
+                    rD[i * nqf + qf] = w * ttc[b * Fq + fq];
+                  }
                 z += w * rhsf[b * Fq + fq];
                 for (int cp = 0; cp < ncomp; ++cp)
                   {
                     const double tw = w * tcW[(b * 3 + cmp_of(cp)) * Fq + fq];
-                    rA[(i * 3 + cp) * nqf + qf] = tw;
+                    if (!RW)
+                      rA[(i * 3 + cp) * nqf + qf] = tw;
                     z += tw * Hs[cp * Fq + fq];
                   }
               }
@@ -1020,8 +1029,18 @@ namespace ddhdg
 #pragma unroll
             for (int qf = 0; qf < nqf; ++qf)
               {
-                wa[qf]  = rA[(i * 3 + cj) * nqf + qf];
-                ws_[qf] = (cj == ci2) ? rS[i * nqf + qf] : 0.;
+                if (RW)
+                  {
+                    const int    fq = fi * nqf + qf, bb = cmp_of(ci2);
+                    const double w  = w_f[fq] * xi[qf * nf + i % nf];
+                    wa[qf]          = w * tcW[(bb * 3 + cmp_of(cj)) * Fq + fq];
+                    ws_[qf]         = (cj == ci2) ? w * tcS[bb * Fq + fq] : 0.;
+                  }
+                else
+                  {
+                    wa[qf]  = rA[(i * 3 + cj) * nqf + qf];
+                    ws_[qf] = (cj == ci2) ? rS[i * nqf + qf] : 0.;
+                  }
               }
 #pragma unroll
             for (int e = 0; e < nb; ++e)
@@ -1099,6 +1118,16 @@ namespace ddhdg
               const int  fi  = i / (ncomp * nf), ci2 = (i / nf) % ncomp;
               const bool rok = dfl[i] == 0.;
               const JT    *rAi = rA + i * 3 * nqf, *rDi = rD + i * nqf;
+              // 3D FP64: the row's face weights, times the coefficients below
+              double wi[nqf];
+              int    bi3 = 0;
+              if (RW)
+                {
+                  bi3 = cmp_of(ci2);
+#pragma unroll
+                  for (int qf = 0; qf < nqf; ++qf)
+                    wi[qf] = w_f[fi * nqf + qf] * xi[qf * nf + i % nf];
+                }
 #pragma unroll
               for (int nt = 0; nt < NNT; ++nt)
 #pragma unroll
@@ -1116,11 +1145,20 @@ namespace ddhdg
                         double    z   = d[nt][e];
 #pragma unroll
                         for (int qf = 0; qf < nqf; ++qf)
-                          z += rAi[ct * nqf + qf] * RQr[(fi * nqf + qf) * Ft + tqq];
+                          {
+                            const double ra =
+                              RW ? wi[qf] * tcW[(bi3 * 3 + cmp_of(ct)) * Fq + fi * nqf + qf]
+                                 : (double)rAi[ct * nqf + qf];
+                            z += ra * RQr[(fi * nqf + qf) * Ft + tqq];
+                          }
                         if (ft == fi && ct == ci2)
 #pragma unroll
                           for (int qf = 0; qf < nqf; ++qf)
-                            z += rDi[qf] * xi[qf * nf + mt];
+                            {
+                              const double rd =
+                                RW ? wi[qf] * ttc[bi3 * Fq + fi * nqf + qf] : (double)rDi[qf];
+                              z += rd * xi[qf * nf + mt];
+                            }
                         o = z;
                       }
                     tt_out[(int64_t)i * Nt + t] = o;
