@@ -1,19 +1,20 @@
-// Per-cell assembly + static condensation, one warp per cell (sm_100a, FP64
-// or with an FP32 Jacobian),
-// for local scalar systems of at most 32 unknowns (3 (k+1)^d <= 32: 2D k <= 2,
-// 3D k = 1, 1D).
+// Per-cell assembly + static condensation, one warp per cell (sm_100a), for
+// local scalar systems of at most 32 unknowns (3 (k+1)^d <= 32: 1D, 2D
+// k <= 2, 3D k = 1), in FP64 or with an FP32 Jacobian (JT = float).
 //
 // Same mathematics as condense2_kernel (hdg_condense.cuh): the flux unknowns
 // are eliminated through the constant mass matrix and the scalar system
 // S y = R of the enabled components is solved for the residual and for every
 // trace dof.  The execution model differs: every lane owns one row of S in
-// registers and the Gauss-Jordan inverse runs as a short loop of warp
-// shuffles (virtual partial pivoting; the register row is rotated by one
-// position per step so that the current column is always register 0);
-// Y = S^-1 R is formed with per-lane register accumulators; and the condensed
-// trace matrix tt = T Y + (face terms) is a register-tiled product on a 4 x 8
-// lane grid.  Warps are independent; the constant tables are read through
-// the L1 cache.
+// registers and the Gauss-Jordan inverse runs as a short loop over the
+// columns (virtual partial pivoting with a warp max-reduction of a packed
+// pivot key; the register row is rotated by one position per step so that
+// the current column is always register 0); Y = S^-1 R and the condensed
+// trace matrix tt = T Y + (face terms) are products on the FP64 tensor path
+// (mma.sync m8n8k4, 8 x 8 tiles), with the face terms added per output in
+// the epilogue.  Warps are independent; the tables used at lane-uniform
+// addresses travel in the constant bank (a __grid_constant__ parameter),
+// the others are read through the L1 cache.
 #pragma once
 
 #include <cstdint>

@@ -16,10 +16,18 @@
 //             W = F_EE^-1 [F_EK | r_E], Schur update F_KK -= F_KE W
 //   downward  x_E = y_E - W x_K from the root to the leaves
 //
-// Fronts of one height and one shape are processed as one batch (cuBLAS
-// batched LU, triangular solves and GEMMs; cuSOLVER dense LU for the few
-// large fronts near the root).  Before the factorisation the rows are
-// equilibrated: row g is scaled by 1 / max |row g| over the cells sharing it.
+// Fronts of one height and one shape are processed as one batch:
+//   <= 36 eliminated dofs   one fused kernel, a CTA per front (LU, W and the
+//                           Schur update)
+//   37..72                  a CTA per front for the LU and W, the Schur update
+//                           as a batched cuBLAS GEMM
+//   up to 383               batched cuBLAS LU, triangular solves and GEMMs
+//   >= 384 (few fronts)     cuSOLVER LU per front, cuBLAS triangular solves
+//                           and GEMM, fronts spread over side streams
+// The numeric sequence is captured in a CUDA graph on the second call with
+// the same buffers and replayed afterwards.  Before the factorisation the
+// rows are equilibrated: row g is scaled by 1 / max |row g| over the cells
+// sharing it.
 #pragma once
 
 #include <cublas_v2.h>
