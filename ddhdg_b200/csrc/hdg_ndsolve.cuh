@@ -444,6 +444,225 @@ namespace ddhdg
       info[blockIdx.x] = sing_s;
   }
 
+  // Dense LU with partial pivoting of F_EE for the fronts of a batch, one
+  // CTA per front (NDLuTPB threads), all fronts of the batch at once; LAPACK
+  // getrf output: L and U in place, ipiv (1-based sequential row swaps),
+  // info = first zero pivot.  Right-looking, panels of NDLuNB columns:
+  // - the panel (rows k0..nE-1) is factorised in shared memory: block-wide
+  //   pivot search, row swap, and a row-owner update of the panel's columns;
+  // - its swaps are applied to the rest of the front's rows in global
+  //   memory (L2-resident), then U12 = L11^-1 A12 is solved column by column
+  //   in registers by the thread that swapped the column;
+  // - the trailing update A22 -= L21 U12 is a register-tiled FP64 product:
+  //   a warp per group of 4 columns and 128-row block (a lane per row, rows
+  //   32 apart), U12 staged in shared memory NDLuCols columns at a time.
+  // For fronts of at most NDLuMaxE eliminated dofs (the panel fits in shared
+  // memory).
+  constexpr int NDLuNB   = 32;
+  constexpr int NDLuCols = 64;
+  constexpr int NDLuTPB  = 512;
+  constexpr int NDLuMaxE = 576;
+
+  __host__ __device__ inline size_t
+  nd_lu_smem(int nE)
+  {
+    return ((size_t)nE * NDLuNB + (size_t)NDLuNB * NDLuCols) * sizeof(double);
+  }
+
+  __global__ void __launch_bounds__(NDLuTPB, 1)
+  nd_lu_front_kernel(int nE, int nF, const NDSol *nodes, int *ipiv_all, int *info, double *fronts)
+  {
+    extern __shared__ double sm[];
+    __shared__ double rv[NDLuTPB / 32];
+    __shared__ int    ri[NDLuTPB / 32];
+    __shared__ int    pv[NDLuNB];
+    __shared__ int    sing_s;
+    constexpr int     NW   = NDLuTPB / 32;
+    const int         tid  = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double           *A    = fronts + nodes[blockIdx.x].off; // F_EE: A[i + c nF]
+    int              *ipiv = ipiv_all + (int64_t)blockIdx.x * nE;
+    double           *Pn   = sm;                       // panel [NDLuNB][nE]: Pn[i + j nE]
+    double           *Us   = sm + (size_t)nE * NDLuNB; // U12 chunk [NDLuNB][NDLuCols]
+    if (tid == 0)
+      sing_s = 0;
+    for (int k0 = 0; k0 < nE; k0 += NDLuNB)
+      {
+        const int w = min(NDLuNB, nE - k0), m = nE - k0;
+        for (int j = 0; j < w; ++j)
+          for (int i = tid; i < m; i += NDLuTPB)
+            Pn[i + j * nE] = A[(int64_t)(k0 + j) * nF + k0 + i];
+        __syncthreads();
+        // ---- panel factorisation
+        for (int j = 0; j < w; ++j)
+          {
+            double best = -1.;
+            int    bi   = m;
+            for (int i = j + tid; i < m; i += NDLuTPB)
+              {
+                const double v = fabs(Pn[i + j * nE]);
+                if (v > best)
+                  {
+                    best = v;
+                    bi   = i;
+                  }
+              }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+              {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int    oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi))
+                  {
+                    best = ob;
+                    bi   = oi;
+                  }
+              }
+            if (lane == 0)
+              {
+                rv[warp] = best;
+                ri[warp] = bi;
+              }
+            __syncthreads();
+            if (warp == 0)
+              {
+                best = lane < NW ? rv[lane] : -1.;
+                bi   = lane < NW ? ri[lane] : m;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+                  {
+                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int    oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ob > best || (ob == best && oi < bi))
+                      {
+                        best = ob;
+                        bi   = oi;
+                      }
+                  }
+                if (lane == 0)
+                  {
+                    const int p  = (bi < m) ? bi : j;
+                    pv[j]        = p;
+                    ipiv[k0 + j] = k0 + p + 1;
+                    if ((!(best > 0.) || !isfinite(best)) && sing_s == 0)
+                      sing_s = k0 + j + 1;
+                  }
+              }
+            __syncthreads();
+            const int p = pv[j];
+            if (p != j && tid < w)
+              {
+                const double t   = Pn[j + tid * nE];
+                Pn[j + tid * nE] = Pn[p + tid * nE];
+                Pn[p + tid * nE] = t;
+              }
+            __syncthreads();
+            const double d  = Pn[j + j * nE];
+            const double hr = (d != 0.) ? 1. / d : 0.;
+            for (int i = j + 1 + tid; i < m; i += NDLuTPB)
+              {
+                const double l = Pn[i + j * nE] * hr;
+                Pn[i + j * nE] = l;
+                for (int c = j + 1; c < w; ++c)
+                  Pn[i + c * nE] -= l * Pn[j + c * nE];
+              }
+            __syncthreads();
+          }
+        for (int j = 0; j < w; ++j)
+          for (int i = tid; i < m; i += NDLuTPB)
+            A[(int64_t)(k0 + j) * nF + k0 + i] = Pn[i + j * nE];
+        // ---- the panel's swaps on the other columns; U12 for the trailing ones
+        for (int c = tid; c < nE; c += NDLuTPB)
+          {
+            if (c >= k0 && c < k0 + w)
+              continue;
+            double *col = A + (int64_t)c * nF;
+            for (int j = 0; j < w; ++j)
+              {
+                const int p = pv[j];
+                if (p != j)
+                  {
+                    const double t = col[k0 + j];
+                    col[k0 + j]    = col[k0 + p];
+                    col[k0 + p]    = t;
+                  }
+              }
+            if (c >= k0 + w)
+              {
+                double x[NDLuNB];
+#pragma unroll
+                for (int r = 0; r < NDLuNB; ++r)
+                  x[r] = (r < w) ? col[k0 + r] : 0.;
+#pragma unroll
+                for (int r = 0; r < NDLuNB; ++r)
+                  if (r < w)
+#pragma unroll
+                    for (int t = r + 1; t < NDLuNB; ++t)
+                      if (t < w)
+                        x[t] -= Pn[t + r * nE] * x[r];
+#pragma unroll
+                for (int r = 0; r < NDLuNB; ++r)
+                  if (r < w)
+                    col[k0 + r] = x[r];
+              }
+          }
+        __syncthreads();
+        // ---- trailing update A22 -= L21 U12
+        const int r0 = k0 + w, nr = nE - r0;
+        for (int cc = r0; cc < nE; cc += NDLuCols)
+          {
+            const int wc = min(NDLuCols, nE - cc);
+            for (int idx = tid; idx < w * wc; idx += NDLuTPB)
+              {
+                const int t = idx % w, c = idx / w;
+                Us[t * NDLuCols + c] = A[(int64_t)(cc + c) * nF + k0 + t];
+              }
+            __syncthreads();
+            for (int g = warp; g < (wc + 3) / 4 * ((nr + 127) / 128); g += NW)
+              {
+                const int cg = g % ((wc + 3) / 4), rb = g / ((wc + 3) / 4);
+                const int c0 = cg * 4;
+                double    acc[4][4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                  for (int q = 0; q < 4; ++q)
+                    acc[r][q] = 0.;
+                for (int t = 0; t < w; ++t)
+                  {
+                    double lv[4], uv[4];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                      {
+                        const int i = rb * 128 + lane + 32 * r; // row of A22
+                        lv[r]       = (i < nr) ? Pn[(w + i) + t * nE] : 0.;
+                      }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                      uv[q] = (c0 + q < wc) ? Us[t * NDLuCols + c0 + q] : 0.;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+#pragma unroll
+                      for (int q = 0; q < 4; ++q)
+                        acc[r][q] += lv[r] * uv[q];
+                  }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                  if (c0 + q < wc)
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                      {
+                        const int i = rb * 128 + lane + 32 * r;
+                        if (i < nr)
+                          A[(int64_t)(cc + c0 + q) * nF + r0 + i] -= acc[r][q];
+                      }
+              }
+            __syncthreads();
+          }
+      }
+    if (tid == 0)
+      info[blockIdx.x] = sing_s;
+  }
+
   // Mid fronts (NDSmallE < nE <= NDMidE), one CTA of 16 warps per front
   // (above 72 eliminated dofs the single-warp diagonal-block solves make it
   // slower than the batched cuBLAS path):
@@ -899,7 +1118,8 @@ namespace ddhdg
       if (allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_front_kernel)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_rowperm_kernel)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_backsolve_kernel)) != cudaSuccess ||
-          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_mid_front_kernel)) != cudaSuccess)
+          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_mid_front_kernel)) != cudaSuccess ||
+          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_lu_front_kernel)) != cudaSuccess)
         return bad(err, "cannot raise the shared-memory limit of the trace-solve kernels", DDHDG_CUDA_ERROR);
       nodes_info_ = (int)nodes_.size();
       built_      = true;
@@ -1066,7 +1286,10 @@ namespace ddhdg
                   info_base += nb;
                   continue;
                 }
-              if (cublasDgetrfBatched(blas_, b.nE, pEE, nF, piv, inf, nb) != CUBLAS_STATUS_SUCCESS)
+              if (b.nE <= NDLuMaxE)
+                nd_lu_front_kernel<<<nb, NDLuTPB, nd_lu_smem(b.nE), s>>>(b.nE, nF, d_sol_ + b.sol_off, piv, inf,
+                                                                        d_fronts_);
+              else if (cublasDgetrfBatched(blas_, b.nE, pEE, nF, piv, inf, nb) != CUBLAS_STATUS_SUCCESS)
                 return bad(err, "cublasDgetrfBatched failed", DDHDG_SOLVER_ERROR);
               // W = U^-1 L^-1 P [F_EK | r_E]: the row permutation by a
               // coalesced in-place gather, then two triangular solves
