@@ -21,7 +21,8 @@
 //                           Schur update)
 //   37..72                  a CTA per front for the LU and W, the Schur update
 //                           as a batched cuBLAS GEMM
-//   up to 383               batched cuBLAS LU, triangular solves and GEMMs
+//   up to 383               own LU, a CTA per front (all fronts at once),
+//                           batched cuBLAS triangular solves and GEMMs
 //   >= 384 (few fronts)     cuSOLVER LU per front, cuBLAS triangular solves
 //                           and GEMM, fronts spread over side streams
 // The numeric sequence is captured in a CUDA graph on the second call with
