@@ -299,11 +299,13 @@ namespace ddhdg
   // W = F_EE^-1 [F_EK | r_E] (written back to the front for the downward
   // pass), then F_KK -= F_KE W in global memory with 4 x 4 register tiles
   // (F_KE read from the front, coalesced over rows).  info[front] = first
-  // zero pivot (1-based) or 0.
+  // zero pivot (1-based) or 0.  Two launch forms of the same body: without a
+  // register cap (the 36-dof fronts), and capped for MINB CTAs per SM (the
+  // smallest fronts of the lowest levels gain from 4 or 5).
   constexpr int NDSmallE = 36;
 
-  __global__ void
-  nd_small_front_kernel(int nE, int nK, const NDSol *nodes, int *info, double *fronts)
+  __device__ __forceinline__ void
+  nd_small_front(int nE, int nK, const NDSol *nodes, int *info, double *fronts)
   {
     extern __shared__ double sm[];
     __shared__ int     piv_s, sing_s;
@@ -443,6 +445,19 @@ namespace ddhdg
     }
     if (tid == 0)
       info[blockIdx.x] = sing_s;
+  }
+
+  __global__ void
+  nd_small_front_kernel(int nE, int nK, const NDSol *nodes, int *info, double *fronts)
+  {
+    nd_small_front(nE, nK, nodes, info, fronts);
+  }
+
+  template <int MINB>
+  __global__ void __launch_bounds__(256, MINB)
+  nd_small_front_capped_kernel(int nE, int nK, const NDSol *nodes, int *info, double *fronts)
+  {
+    nd_small_front(nE, nK, nodes, info, fronts);
   }
 
   // Dense LU with partial pivoting of F_EE for the fronts of a batch, one
@@ -1117,6 +1132,8 @@ namespace ddhdg
           cusolverDnSetStream(side_dn_[k], side_[k]);
         }
       if (allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_front_kernel)) != cudaSuccess ||
+          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_front_capped_kernel<4>)) != cudaSuccess ||
+          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_front_capped_kernel<5>)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_rowperm_kernel)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_backsolve_kernel)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_mid_front_kernel)) != cudaSuccess ||
@@ -1260,8 +1277,15 @@ namespace ddhdg
               int     *inf = d_info_ + info_base;
               if (b.small)
                 {
-                  nd_small_front_kernel<<<nb, 256, small_smem(b.nE, b.nK), s>>>(
-                    b.nE, b.nK, d_sol_ + b.sol_off, d_info_ + info_base, d_fronts_);
+                  // register caps by front shape (measured per tree level on
+                  // the 256 x 256 degree-2 diode)
+                  const size_t sm = small_smem(b.nE, b.nK);
+                  if (b.nE <= 18 && b.nK <= 72)
+                    nd_small_front_capped_kernel<5><<<nb, 256, sm, s>>>(b.nE, b.nK, d_sol_ + b.sol_off, inf, d_fronts_);
+                  else if (b.nE <= 18)
+                    nd_small_front_capped_kernel<4><<<nb, 256, sm, s>>>(b.nE, b.nK, d_sol_ + b.sol_off, inf, d_fronts_);
+                  else
+                    nd_small_front_kernel<<<nb, 256, sm, s>>>(b.nE, b.nK, d_sol_ + b.sol_off, inf, d_fronts_);
                   info_base += nb;
                   continue;
                 }
