@@ -278,9 +278,45 @@ def run_bias_sweep(args):
     def keep(v, s, r):
         points.append({"bias": round(v, 3), "iterations": r.iterations, "converged": bool(r.converged)})
 
-    cases.bias_sweep(g, pb, biases, 1e-10, 1e-10, 50, callback=keep)
-    torch.cuda.synchronize()
-    t_sweep = time.perf_counter() - t0
+    if not args.mixed:
+        cases.bias_sweep(g, pb, biases, 1e-10, 1e-10, 50, callback=keep)
+        torch.cuda.synchronize()
+        t_sweep = time.perf_counter() - t0
+    else:
+        # the same sweep with the mixed-precision condensation, in lockstep
+        # from the same equilibrium state: every point's final V, n, p against
+        # the FP64 sweep's (largest difference per component block, relative
+        # to the block's largest magnitude)
+        pbm, prmm, adimm = cases.diode(dim=WORKLOAD["dim"], m=m_side, k=WORKLOAD["k"],
+                                       length=m_side / WORKLOAD["m"], precision=1)
+        prmm.consistent_drift_jacobian = True
+        prmm.consistent_recombination_jacobian = True
+        gm = NPSolver(pbm, prmm, adimm)
+        gm.set_state(g.get_cell_state(), g.get_trace_state())
+        d, nb = WORKLOAD["dim"], (WORKLOAD["k"] + 1) ** WORKLOAD["dim"]
+        t_sweep = t_mixed = 0.0
+        for v in biases:
+            tp = time.perf_counter()
+            cases.set_bias(pb, v)
+            g.update_boundary_tables()
+            r = g.run(1e-10, 1e-10, 50)
+            torch.cuda.synchronize()
+            t_sweep += time.perf_counter() - tp
+            tp = time.perf_counter()
+            cases.set_bias(pbm, v)
+            gm.update_boundary_tables()
+            rm = gm.run(1e-10, 1e-10, 50)
+            torch.cuda.synchronize()
+            t_mixed += time.perf_counter() - tp
+            c64, t64, c32, t32 = g.get_cell_state(), g.get_trace_state(), gm.get_cell_state(), gm.get_trace_state()
+            err = 0.0
+            for c in range(3):
+                ia = slice(c * (d + 1) * nb, (c + 1) * (d + 1) * nb)
+                for x, y in ((c32[:, ia], c64[:, ia]), (t32[:, c], t64[:, c])):
+                    err = max(err, float(np.abs(x - y).max() / max(np.abs(y).max(), 1e-300)))
+            points.append({"bias": round(v, 3), "iterations": r.iterations, "converged": bool(r.converged),
+                           "mixed_iterations": rm.iterations, "mixed_converged": bool(rm.converged),
+                           "mixed_vs_fp64_rel_diff": err})
     steps = sum(p["iterations"] for p in points)
     line = {"metric": "bias sweep wall time (17 points, warm-started Newton)", "value": t_sweep, "unit": "s",
             "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
@@ -288,6 +324,11 @@ def run_bias_sweep(args):
                        "trace_dofs": int(g.sizes().n_trace_dofs), "cells": g.ncells},
             "equilibrium_s": t_eq, "equilibrium_iterations": req.iterations,
             "newton_steps": steps, "ms_per_newton_step": 1e3 * t_sweep / max(steps, 1), "points": points}
+    if args.mixed:
+        msteps = sum(p["mixed_iterations"] for p in points)
+        line["mixed"] = {"sweep_s": t_mixed, "newton_steps": msteps,
+                         "ms_per_newton_step": 1e3 * t_mixed / max(msteps, 1),
+                         "max_rel_diff_vs_fp64": max(p["mixed_vs_fp64_rel_diff"] for p in points)}
     print(json.dumps(line))
 
 
@@ -419,6 +460,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=4.0, help="arrivals per second")
     ap.add_argument("--bias-sweep", action="store_true",
                     help="time the warm-started 0..0.8 V sweep (17 points) instead of the step")
+    ap.add_argument("--mixed", action="store_true",
+                    help="with --bias-sweep: the same sweep with the mixed-precision condensation, compared point by point")
     ap.add_argument("--trace-solve", action="store_true",
                     help="time the global trace solve alone (nested dissection) on the diode's condensed system")
     ap.add_argument("--condense-3d", action="store_true",
