@@ -57,3 +57,36 @@ def test_ctx_create_without_device_fails_cleanly():
     ctx = ctypes.c_void_p()
     assert L.ddhdg_ctx_create(ctypes.byref(D), ctypes.byref(ctx)) != 0
     assert not ctx
+
+
+def test_argument_checks_before_any_device_work():
+    """Null contexts and invalid descriptors are rejected with a bad-argument
+    status and a message, before any CUDA call (so also on a machine without
+    a GPU): the host-buffer calls, the trace solve and its graph switch; a
+    precision other than 0 / 1, mixed precision where no FP32 kernel exists
+    (2D degree 3), and meshes of 2^31 cells or more."""
+    L = _lib.load(build_if_missing=False)
+    vp = ctypes.c_void_p
+    null = vp()
+    assert L.ddhdg_set_solver_graphs(null, 1) == 1
+    assert L.ddhdg_assemble_condense_host(null, null, null, 0, null, null, null, null, null) == 1
+    assert L.ddhdg_reconstruct_host(null, null, 0, null, null) == 1
+    assert L.ddhdg_solve_condensed(null, null, null, null, null, null, 0, null) == 1
+
+    def create(**kw):
+        D = _lib.ProblemDesc()
+        D.dim, D.degree = kw.get("dim", 2), kw.get("degree", 1)
+        for a in range(3):
+            D.n[a] = kw.get("n", 4)
+            D.h[a] = 1.0
+        D.precision = kw.get("precision", 0)
+        ctx = vp()
+        rc = L.ddhdg_ctx_create(ctypes.byref(D), ctypes.byref(ctx))
+        return rc, L.ddhdg_last_error().decode()
+
+    rc, msg = create(precision=2)
+    assert rc == 1 and "precision" in msg
+    rc, msg = create(degree=3, precision=1)
+    assert rc == 1 and "mixed precision" in msg
+    rc, msg = create(n=50000)
+    assert rc == 1 and "2^31" in msg
