@@ -679,6 +679,144 @@ namespace ddhdg
       info[blockIdx.x] = sing_s;
   }
 
+  // Small fronts above the leaves, whole front in shared memory: the front
+  // is assembled there from its two children's Schur complements (the
+  // extend-add), eliminated there (LU with partial pivoting of F_EE,
+  // W = F_EE^-1 [F_EK | r_E], F_KK -= F_KE W), and only its columns
+  // nE..nF (W and the kept block with the kept rhs) are written to the
+  // front in global memory: no zeroing of the front, no extend-add through
+  // global memory, no second read.  One CTA per front; used where the front
+  // (nF x (nF + 1) doubles) takes at most 100 KB of shared memory (two CTAs
+  // per SM or more: with one, the 126-dof fronts ran slower than the
+  // unfused path).
+  __host__ __device__ inline size_t
+  nd_fused_smem(int nF)
+  {
+    return (size_t)nF * (nF + 1) * sizeof(double);
+  }
+
+  __global__ void __launch_bounds__(256)
+  nd_small_fused_kernel(int nE, int nK, const NDAsm *asmn, const int32_t *emap, int *info, double *fronts)
+  {
+    extern __shared__ double F[]; // [nF + 1 columns][nF rows], column-major
+    __shared__ int     piv_s, sing_s;
+    const int          nF = nE + nK, nc = nK + 1;
+    const NDAsm        nd = asmn[blockIdx.x];
+    const int          tid = threadIdx.x, T = blockDim.x;
+    for (int idx = tid; idx < nF * (nF + 1); idx += T)
+      F[idx] = 0.;
+    if (tid == 0)
+      sing_s = 0;
+    __syncthreads();
+    // extend-add of the two children (they overlap: one after the other)
+    for (int s = 0; s < 2; ++s)
+      {
+        const int      cnF = nd.cnF[s], cnE = nd.cnE[s], cnK = cnF - cnE;
+        const double  *Fc  = fronts + nd.coff[s];
+        const int32_t *map = emap + nd.moff[s];
+        const int      tot = (cnK + 1) * cnK;
+        for (int e = tid; e < tot; e += T)
+          {
+            const int j = e / cnK, i = e - j * cnK;
+            const int pj = (j < cnK) ? map[j] : nF;
+            F[pj * nF + map[i]] += Fc[(int64_t)(cnE + j) * cnF + cnE + i];
+          }
+        __syncthreads();
+      }
+    // LU of F_EE with the row swaps and updates carried across all columns
+    for (int j = 0; j < nE; ++j)
+      {
+        if (tid < 32)
+          {
+            double best = -1.;
+            int    bi   = nE;
+            for (int i = j + tid; i < nE; i += 32)
+              {
+                const double v = fabs(F[i + j * nF]);
+                if (v > best)
+                  {
+                    best = v;
+                    bi   = i;
+                  }
+              }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+              {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int    oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi))
+                  {
+                    best = ob;
+                    bi   = oi;
+                  }
+              }
+            if (tid == 0)
+              {
+                piv_s = (bi < nE) ? bi : j;
+                if ((!(best > 0.) || !isfinite(best)) && sing_s == 0)
+                  sing_s = j + 1;
+              }
+          }
+        __syncthreads();
+        const int p = piv_s;
+        if (p != j)
+          for (int c = tid; c <= nF; c += T)
+            {
+              const double t = F[j + c * nF];
+              F[j + c * nF]  = F[p + c * nF];
+              F[p + c * nF]  = t;
+            }
+        __syncthreads();
+        const double d  = F[j + j * nF];
+        const double hr = (d != 0.) ? 1. / d : 0.;
+        for (int i = j + 1 + tid; i < nE; i += T)
+          F[i + j * nF] *= hr;
+        __syncthreads();
+        const int nr = nE - j - 1;
+        if (nr > 0)
+          for (int idx = tid; idx < nr * (nF - j); idx += T)
+            {
+              const int i = j + 1 + idx % nr, c = j + 1 + idx / nr;
+              F[i + c * nF] -= F[i + j * nF] * F[j + c * nF];
+            }
+        __syncthreads();
+      }
+    // back substitution with U on the columns nE..nF (W)
+    for (int j = nE - 1; j >= 0; --j)
+      {
+        const double d  = F[j + j * nF];
+        const double hr = (d != 0.) ? 1. / d : 0.;
+        for (int c = nE + tid; c <= nF; c += T)
+          F[j + c * nF] *= hr;
+        __syncthreads();
+        if (j > 0)
+          for (int idx = tid; idx < j * nc; idx += T)
+            {
+              const int i = idx % j, c = nE + idx / j;
+              F[i + c * nF] -= F[i + j * nF] * F[j + c * nF];
+            }
+        __syncthreads();
+      }
+    // Schur update of the kept rows (F_KE and W are only read here)
+    for (int idx = tid; idx < nK * nc; idx += T)
+      {
+        const int i = nE + idx % nK, c = nE + idx / nK;
+        double    acc = 0.;
+        for (int k = 0; k < nE; ++k)
+          acc += F[i + k * nF] * F[k + c * nF];
+        F[i + c * nF] -= acc;
+      }
+    __syncthreads();
+    double *Fv = fronts + nd.off;
+    for (int idx = tid; idx < nF * nc; idx += T)
+      {
+        const int i = idx % nF, c = nE + idx / nF;
+        Fv[(int64_t)c * nF + i] = F[i + c * nF];
+      }
+    if (tid == 0)
+      info[blockIdx.x] = sing_s;
+  }
+
   // Mid fronts (NDSmallE < nE <= NDMidE), one CTA of 16 warps per front
   // (above 72 eliminated dofs the single-warp diagonal-block solves make it
   // slower than the batched cuBLAS path):
@@ -1064,6 +1202,7 @@ namespace ddhdg
           b.big   = b.nE >= 384 && b.nodes.size() <= 32;
           b.small = !b.big && b.nE > 0 && b.nE <= NDSmallE && small_smem(b.nE, b.nK) <= 200 * 1024;
           b.mid   = !b.big && !b.small && b.nE > 0 && b.nE <= NDMidE && nd_mid_smem(b.nE) <= 220 * 1024;
+          b.fused = b.small && b.height > 0 && nd_fused_smem(b.nE + b.nK) <= 100 * 1024;
           max_nK_ = std::max(max_nK_, b.nK);
         }
       return DDHDG_OK;
@@ -1137,6 +1276,7 @@ namespace ddhdg
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_rowperm_kernel)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_backsolve_kernel)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_mid_front_kernel)) != cudaSuccess ||
+          allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_fused_kernel)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_lu_front_kernel)) != cudaSuccess)
         return bad(err, "cannot raise the shared-memory limit of the trace-solve kernels", DDHDG_CUDA_ERROR);
       nodes_info_ = (int)nodes_.size();
@@ -1254,7 +1394,7 @@ namespace ddhdg
         {
           const int nF = b.nE + b.nK;
           const int nb = (int)b.nodes.size();
-          if (b.height > 0)
+          if (b.height > 0 && !b.fused)
             {
               if (cudaMemsetAsync(d_fronts_ + b.front_off, 0,
                                   (b.front_end - b.front_off) * sizeof(double), s) != cudaSuccess)
@@ -1275,6 +1415,13 @@ namespace ddhdg
               double **pEE = d_ptr_ + b.ptr_off, **pEK = pEE + nb, **pKE = pEK + nb, **pKK = pKE + nb;
               int     *piv = d_piv_ + b.piv_off;
               int     *inf = d_info_ + info_base;
+              if (b.fused)
+                {
+                  nd_small_fused_kernel<<<nb, 256, nd_fused_smem(nF), s>>>(b.nE, b.nK, d_asm_ + b.asm_off, d_emap_,
+                                                                          inf, d_fronts_);
+                  info_base += nb;
+                  continue;
+                }
               if (b.small)
                 {
                   // register caps by front shape (measured per tree level on
@@ -1398,6 +1545,7 @@ namespace ddhdg
       int              maxc[2] = {0, 0}; // max child nK + 1 per extend-add pass
       bool             small   = false;  // fused one-CTA elimination
       bool             mid     = false;  // one-CTA LU + W, batched GEMM Schur update
+      bool             fused   = false;  // small, assembled and eliminated in shared memory
     };
 
     static size_t
