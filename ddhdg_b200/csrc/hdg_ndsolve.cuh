@@ -18,7 +18,8 @@
 //
 // Fronts of one height and one shape are processed as one batch:
 //   <= 36 eliminated dofs   one fused kernel, a CTA per front (LU, W and the
-//                           Schur update)
+//                           Schur update); above the leaves, while the front
+//                           fits, it is also assembled in shared memory
 //   37..72                  a CTA per front for the LU and W, the Schur update
 //                           as a batched cuBLAS GEMM
 //   up to 383               own LU, a CTA per front (all fronts at once),
