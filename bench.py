@@ -96,10 +96,37 @@ def fp64_peak_tflops(dev):
     return 3 * 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
 
 
-# DRAM bytes (read + write) of one condense launch per cell, from the ncu
-# capture summarised in profiles/condense3_2d_k2.md (16 384 cells: 14.8 MB
-# read + 260.6 MB written), scaled to a launch by the cells it processes
-TRAFFIC_BYTES_PER_CELL = 16806
+# DRAM bytes (read + write) per cell of one launch of the FP64 condense
+# kernel, measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on
+# the 128 x 128 mesh of the same diode and scaled to a launch by the cells it
+# processes.  The figure belongs to one version of the kernel source: it is
+# reported only while the sha256 of hdg_condense3.cuh matches, else null.
+TRAFFIC = {"bytes_per_cell": 16806, "kernel_source": "ddhdg_b200/csrc/hdg_condense3.cuh",
+           "kernel_sha256": None}
+
+
+def traffic_bytes_per_cell():
+    import hashlib
+
+    if not TRAFFIC["kernel_sha256"]:
+        return None
+    try:
+        with open(os.path.join(ROOT, TRAFFIC["kernel_source"]), "rb") as f:
+            sha = hashlib.sha256(f.read()).hexdigest()
+    except OSError:
+        return None
+    return TRAFFIC["bytes_per_cell"] if sha == TRAFFIC["kernel_sha256"] else None
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def bytes_per_cell(dim, k, ncomp=3):
@@ -168,17 +195,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(k_sample_cells=4096, steps=1):
+def cpu_baseline(k_sample_cells=4096, steps=1, nthreads=None):
     """The oracle (the reference's per-cell algorithm restated in C++,
-    OpenMP over cells) on a 64 x 64 slab of the same diode (same cell size,
-    degree and physics): assembly + condensation + reconstruction."""
+    OpenMP over cells) on a slab of the same diode (same cell size, degree
+    and physics; 64 x 64 cells by default): assembly + condensation +
+    reconstruction."""
     from oracle.oracle import OracleSolver
     from ddhdg_b200 import workloads as cases
 
     m_side = int(round(k_sample_cells ** 0.5))
     length = m_side / WORKLOAD["m"]
     pb, prm, adim = cases.diode(dim=WORKLOAD["dim"], m=m_side, k=WORKLOAD["k"], length=length)
-    o = OracleSolver(pb, prm, adim, nthreads=os.cpu_count() or 1)
+    cores = nthreads or os.cpu_count() or 1
+    o = OracleSolver(pb, prm, adim, nthreads=cores)
     o.compute_local_charge_neutrality()
     o.project_quasi_fermi(1)
     o.project_quasi_fermi(2)
@@ -190,8 +219,8 @@ def cpu_baseline(k_sample_cells=4096, steps=1):
         o.reconstruct(upd)
         dt = time.perf_counter() - t0
         best = dt if best is None else min(best, dt)
-    return {"value": o.ncells / best, "unit": "cells/s", "cores": os.cpu_count() or 1,
-            "kind": "port",
+    return {"value": o.ncells / best, "unit": "cells/s", "cores": cores,
+            "kind": "port", "cells": o.ncells, "ms_per_sample": best * 1e3, "cpu_model": cpu_model(),
             "sample": f"{m_side}x{m_side} cells of the 256x256 k=2 diode (same cell size), "
                       f"assembly+condensation+reconstruction, {o.ncells} cells per step"}
 
@@ -208,13 +237,20 @@ def run_reference(args):
         info = cpu_baseline(steps=1)
         steps.append(info["value"])
     v = float(np.median(steps))
+    single = cpu_baseline(k_sample_cells=256, steps=1, nthreads=1)
     line = {
         "impl": "reference", "metric": "HDG cells condensed/s (assemble+condense+reconstruct)",
         "value": v, "unit": "cells/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 65536 / v * 1e3, "higher_is_better": True, "scaling": "weak",
+        # what one timed step processed: the bounded 64 x 64 sample
+        "ms_per_step": info["cells"] / v * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "2D p-n diode 256x256 quads, HDG degree 2, FP64 (bounded host sample)",
-                   "cells": 65536},
+        "config": {"workload": "2D p-n diode, HDG degree 2, FP64, cell size 1/256 um: a 64x64-cell sample "
+                               "of the 256x256 mesh per step (cells are independent, so cells/s carries over)",
+                   "cells": info["cells"], "full_mesh_cells": 65536},
+        "ms_per_cell": 1e3 / v,
+        "full_mesh_ms_estimate": 65536 / v * 1e3,
+        "cpu_model": info["cpu_model"],
+        "single_thread": {"value": single["value"], "unit": "cells/s", "cells": single["cells"]},
         "cpu_baseline": dict(info, value=v),
         "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -249,6 +285,26 @@ def run_serve(args):
             "solves_per_s": st["solves_per_s"], "cells_per_s": st["cells_per_s"],
             "converged": st["converged"], "peak_inflight": server.peak_inflight, "wall_s": wall}
     print(json.dumps(line))
+
+
+def serve_quick(n=10, rate=4.0, seed=7):
+    """A short seeded Poisson stream of small diode solves through the
+    serving layer (2D 32^2..96^2 at degree 1-2, 3D 8^3..12^3 at degree 1):
+    p50 / p99 latency and solves/s, for the default bench line."""
+    from ddhdg_b200 import serving
+
+    serving.solve_one(serving.Request(-1, 2, 32, 1, 0.1, 0.0))  # warm the kernels
+    reqs = serving.poisson_requests(n, rate, seed=seed, sizes_2d=(32, 96), sizes_3d=(8, 12))
+    server = serving.DiodeServer(max_inflight=8)
+    t0 = time.perf_counter()
+    res = server.run(reqs)
+    wall = time.perf_counter() - t0
+    st = serving.latency_stats(res, wall)
+    return {"p50_s": st["p50_s"], "p99_s": st["p99_s"], "solves_per_s": st["solves_per_s"],
+            "converged": st["converged"], "requests": n, "rate_per_s": rate, "seed": seed,
+            "peak_inflight": server.peak_inflight, "wall_s": wall,
+            "workload": "Poisson stream of 2D 32^2..96^2 (k 1-2) and 3D 8^3..12^3 (k 1) diode solves, "
+                        "bias U[0, 0.8] V (full-size stream: bench.py --serve)"}
 
 
 def run_bias_sweep(args):
@@ -454,6 +510,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the short serving stream of the default line")
     ap.add_argument("--serve", action="store_true",
                     help="serve a seeded Poisson stream of diode solves and report p50/p99 latency")
     ap.add_argument("--serve-requests", type=int, default=24)
@@ -640,6 +697,42 @@ def main():
         del gm
         torch.cuda.empty_cache()
 
+    # ---- the plain FP64 GPU path (the reference's per-cell algorithm as
+    # written: full local system, LU of cc per cell, Schur complement; the
+    # reconstruction assembles the cell systems again and solves them) on
+    # the same state
+    psteps = max(3, min(args.steps, 20))
+
+    def condense_p():
+        _lib.check(L.ddhdg_assemble_condense_plain(g._ctx, g.cell_state.data_ptr(), g.trace_state.data_ptr(), 0,
+                                                   tt.data_ptr(), rhs.data_ptr(), dflag.data_ptr(),
+                                                   dval.data_ptr(), sp), "condense (plain)")
+
+    def reconstruct_p():
+        _lib.check(L.ddhdg_reconstruct_plain(g._ctx, g.cell_state.data_ptr(), g.trace_state.data_ptr(),
+                                             dtrace.data_ptr(), dcell.data_ptr(), 0, sp), "reconstruct (plain)")
+
+    for _ in range(max(args.warmup, 3)):
+        condense_p()
+        reconstruct_p()
+    torch.cuda.synchronize()
+    evp = [torch.cuda.Event(enable_timing=True) for _ in range(3 * psteps)]
+    replicas.barrier()
+    torch.cuda.synchronize()
+    for i in range(psteps):
+        evp[3 * i].record(stream)
+        condense_p()
+        evp[3 * i + 1].record(stream)
+        reconstruct_p()
+        evp[3 * i + 2].record(stream)
+    torch.cuda.synchronize()
+    pc = replicas.max_over_ranks(float(np.mean([evp[3 * i].elapsed_time(evp[3 * i + 1]) for i in range(psteps)])), dev)
+    pr = replicas.max_over_ranks(float(np.mean([evp[3 * i + 1].elapsed_time(evp[3 * i + 2]) for i in range(psteps)])), dev)
+    plain = {"condense_ms": pc, "reconstruct_ms": pr, "steps": psteps,
+             "cells_per_s": replicas.job_throughput(nc, pc + pr),
+             "kernel": "plain_kernel<2,2> (81x81 cell system assembled term by term, row-equilibrated LU "
+                       "with partial pivoting, Schur complement; reconstruction: second assembly + solve)"}
+
     # ---- one whole Newton step (BASELINE's second metric): assembly +
     # condensation, nested-dissection trace solve, reconstruction, norms and
     # update, state on the device.  The consistent Jacobian keeps the
@@ -669,6 +762,31 @@ def main():
     del gn
     torch.cuda.empty_cache()
 
+    # ---- the north-star comparison: condensation per Newton step of the
+    # mixed-precision and FP64 block-eliminated paths against the plain FP64
+    # GPU path, and the whole Newton step (the trace solve is the same in all)
+    fp64_c = float(np.mean(cond_ms))
+    fp64_r = float(np.mean(rec_ms))
+    solve_ms = newton["stages_ms"]["trace_solve"]
+    target = {"condense_ms": {"plain_fp64": pc, "fp64": fp64_c},
+              "condense_speedup_vs_plain": {"fp64": pc / fp64_c},
+              "newton_step_ms": {"plain_fp64": pc + solve_ms + pr, "fp64": fp64_c + solve_ms + fp64_r},
+              "note": "Newton-step figures add the measured trace solve (same solver in every path) to each "
+                      "path's measured condense and reconstruct times"}
+    if mixed is not None:
+        target["condense_ms"]["mixed"] = mixed["condense_ms"]
+        target["condense_speedup_vs_plain"]["mixed"] = pc / mixed["condense_ms"]
+        target["newton_step_ms"]["mixed"] = mixed["condense_ms"] + solve_ms + mixed["reconstruct_ms"]
+    base = target["newton_step_ms"]["plain_fp64"]
+    target["newton_step_speedup_vs_plain"] = {k: base / v for k, v in target["newton_step_ms"].items()
+                                              if k != "plain_fp64"}
+
+    # ---- a short seeded serving stream (continuous batching of diode
+    # solves): p50 / p99 latency and solves/s
+    serve = None
+    if world == 1 and not args.no_serve:
+        serve = serve_quick()
+
     fp64_peak = fp64_peak_tflops(dev)
     if rank == 0:
         hbm_peak, peak_kind = peaks()
@@ -691,7 +809,7 @@ def main():
             "stages_ms": {"condense": cond_avg, "reconstruct": float(np.mean(rec_ms))},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp64_peak,
-                         "traffic": (TRAFFIC_BYTES_PER_CELL * nc) if TRAFFIC_BYTES_PER_CELL else None,
+                         "traffic": (tbc * nc) if (tbc := traffic_bytes_per_cell()) else None,
                          "kernel": "condense3_kernel<2,2>",
                          "peak_source": "cuBLAS DGEMM 8192^3 timed in this run",
                          "algorithmic_flops_per_cell": fa,
@@ -704,6 +822,9 @@ def main():
                     "d2h_bytes_per_step": d2h},
             "newton_step": newton,
             "mixed": mixed,
+            "plain": plain,
+            "target": target,
+            "serve": serve,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }

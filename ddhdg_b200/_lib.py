@@ -28,7 +28,8 @@ EXPORTS = [
     "ddhdg_project_cell", "ddhdg_project_trace", "ddhdg_project_density",
     "ddhdg_reference_points", "ddhdg_last_error", "ddhdg_assemble_condense_noalloc",
     "ddhdg_solve_condensed", "ddhdg_assemble_condense_host", "ddhdg_reconstruct_host",
-    "ddhdg_set_solver_graphs",
+    "ddhdg_set_solver_graphs", "ddhdg_local_cell_system", "ddhdg_assemble_condense_plain",
+    "ddhdg_reconstruct_plain", "ddhdg_sample_points",
 ]
 
 
@@ -95,6 +96,11 @@ def load(build_if_missing: bool = True):
     L.ddhdg_assemble_condense_host.argtypes = L.ddhdg_assemble_condense.argtypes
     L.ddhdg_reconstruct_host.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p]
     L.ddhdg_set_solver_graphs.argtypes = [c_void_p, c_int]
+    L.ddhdg_local_cell_system.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int64, c_void_p,
+                                          c_int64] + [c_void_p] * 7
+    L.ddhdg_assemble_condense_plain.argtypes = L.ddhdg_assemble_condense.argtypes
+    L.ddhdg_reconstruct_plain.argtypes = L.ddhdg_reconstruct.argtypes
+    L.ddhdg_sample_points.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_int, c_void_p, c_void_p]
     L.ddhdg_newton.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, c_int,
                                c_double, P(c_int), P(c_double), c_void_p]
     L.ddhdg_last_timings.argtypes = [c_void_p, P(c_double), P(c_double), P(c_double), P(c_int)]

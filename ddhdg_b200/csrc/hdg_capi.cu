@@ -25,6 +25,7 @@
 #include "hdg_condense3.cuh"
 #include "hdg_kernels.cuh"
 #include "hdg_ndsolve.cuh"
+#include "hdg_plain.cuh"
 #include "hdg_tables.h"
 
 using namespace ddhdg;
@@ -143,6 +144,8 @@ struct ddhdg_ctx
   int                t_steps    = 0;
   DevBuf<double>     norm_buf;
   DevBuf<int64_t>    d_face_cells, d_face_local;
+  // the plain (full local system) path: per-CTA workspace and tc slices
+  DevBuf<double>     plain_ws, plain_tc;
   // host-buffer calls: device copies of the state and of the reconstruction
   // input and output, a copy stream per direction, events per chunk
   struct HostIO
@@ -1786,7 +1789,10 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
     set_mode_comps(c, thermo); // host bookkeeping only; no trace sparsity needed here
   CondenseKernel cf;
   ReconstructFn rf;
-  if (!kernels_for(c->dim, c->k, cf, rf))
+  // the same kernel as ddhdg_assemble_condense: the FP32-Jacobian variant on
+  // a mixed-precision context
+  const bool mixed = c->desc.precision == 1;
+  if (!kernels_for(c->dim, c->k, cf, rf, mixed))
     return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
   int     r;
   KParams P     = make_params(c, thermo);
@@ -1803,9 +1809,9 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
   bool          r_global = false;
   if (3 * c->nb <= 32)
     {
-      const Ws3Off w   = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol);
+      const Ws3Off w   = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, mixed ? 4 : 8);
       const size_t per = (size_t)w.total * sizeof(double);
-      int          wpb = (int)std::min<size_t>(Condense3MaxWPB, (220 * 1024) / per);
+      int          wpb = (int)std::min<size_t>(Condense3MaxWPB, (mixed ? 110 : 220) * 1024 / per);
       if (wpb < 1)
         return fail(DDHDG_BAD_ARG, "the per-cell workspace does not fit in shared memory");
       P.wpb   = wpb;
@@ -1830,7 +1836,7 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cf.fn, threads, smem));
   if (per_sm < 1)
     return fail(DDHDG_BAD_ARG, "condense kernel does not fit on an SM");
-  const int grid = (int)std::min<int64_t>(units, (int64_t)per_sm * c->sm_count);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(units, (int64_t)per_sm * c->sm_count));
 
   // scratch: Y cache [ncells][Ns][ycols], then (256-byte aligned) one R block
   // [Ns][ncol] per CTA when R lives outside shared memory
@@ -1854,6 +1860,292 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
   cf.launch(c->T, P, grid, threads, smem, (cudaStream_t)stream);
   CK(cudaGetLastError());
   return DDHDG_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// The plain path: the reference's per-cell algorithm as written (full local
+// system, LU of cc, Schur complement), and the per-cell probe.
+
+namespace
+{
+  struct PlainKernel
+  {
+    const void *fn_smem = nullptr, *fn_glob = nullptr;
+    void (*launch)(bool, const KParams &, const PlainArgs &, int, size_t, cudaStream_t) = nullptr;
+  };
+
+  template <int D, int K>
+  void
+  launch_plain(bool glob, const KParams &P, const PlainArgs &A, int grid, size_t smem, cudaStream_t s)
+  {
+    if (glob)
+      plain_kernel<D, K, true><<<grid, PlainTPB, 0, s>>>(P, A);
+    else
+      plain_kernel<D, K, false><<<grid, PlainTPB, smem, s>>>(P, A);
+  }
+
+  template <int D, int K>
+  void
+  pick_plain(PlainKernel &pk)
+  {
+    pk.fn_smem = reinterpret_cast<const void *>(plain_kernel<D, K, false>);
+    pk.fn_glob = reinterpret_cast<const void *>(plain_kernel<D, K, true>);
+    pk.launch  = launch_plain<D, K>;
+  }
+
+  bool
+  plain_for(int dim, int k, PlainKernel &pk)
+  {
+    switch (dim * 10 + k)
+      {
+        case 11: pick_plain<1, 1>(pk); return true;
+        case 12: pick_plain<1, 2>(pk); return true;
+        case 13: pick_plain<1, 3>(pk); return true;
+        case 21: pick_plain<2, 1>(pk); return true;
+        case 22: pick_plain<2, 2>(pk); return true;
+        case 23: pick_plain<2, 3>(pk); return true;
+        case 31: pick_plain<3, 1>(pk); return true;
+        case 32: pick_plain<3, 2>(pk); return true;
+        default: return false;
+      }
+  }
+
+  // one launch of the plain kernel over `units` cells (or listed cells)
+  int
+  plain_run(ddhdg_ctx *c, int thermo, KParams &P, PlainArgs &A, int64_t units, cudaStream_t s)
+  {
+    PlainKernel pk;
+    if (!plain_for(c->dim, c->k, pk))
+      return fail(DDHDG_BAD_ARG, "unsupported dim/degree");
+    Mode          &m    = c->mode[thermo];
+    const PlainOff wo   = plain_layout(c->dim, c->nb, c->nf, m.ncomp, A.mode);
+    const size_t   ws_b = (size_t)wo.total * sizeof(double);
+    const bool     glob = ws_b > 220 * 1024;
+    const void    *fn   = glob ? pk.fn_glob : pk.fn_smem;
+    const size_t   smem = glob ? 0 : ws_b;
+    if (!glob)
+      CK(allow_full_dynamic_smem(fn));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PlainTPB, smem));
+    if (per_sm < 1)
+      return fail(DDHDG_BAD_ARG, "plain kernel does not fit on an SM");
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(units, (int64_t)per_sm * c->sm_count));
+    int       r;
+    if (A.mode != PlainReconstruct)
+      {
+        if ((r = c->plain_tc.alloc((size_t)grid * wo.Nt * wo.Nc)))
+          return r;
+        A.tcscratch = c->plain_tc.p;
+      }
+    if (glob)
+      {
+        A.wstride = ((int64_t)wo.total + 31) & ~(int64_t)31;
+        if ((r = c->plain_ws.alloc((size_t)grid * A.wstride)))
+          return r;
+        A.wscratch = c->plain_ws.p;
+      }
+    pk.launch(glob, P, A, grid, smem, s);
+    CK(cudaGetLastError());
+    return DDHDG_OK;
+  }
+
+  int
+  plain_prepare(ddhdg_ctx *c, int thermo)
+  {
+    Mode &m = c->mode[thermo];
+    if (!m.built)
+      set_mode_comps(c, thermo); // host bookkeeping only; no trace sparsity needed here
+    return DDHDG_OK;
+  }
+} // namespace
+
+namespace
+{
+  struct SampleArgs
+  {
+    int     dim, k, nb, n[3];
+    double  origin[3], h[3], gl[4];
+    int     what; // 0 V, 1 n, 2 p (physical units); 3 phi_n, 4 phi_p (volts)
+    double  V_rescale, n_rescale, T, ec, ev, nc, nv;
+    int64_t npoints;
+  };
+
+  // get_solution_on_a_point (src/np_solver.cpp:1637-1700) for a batch of
+  // points: the cell holding each point (on an interior face the cell above
+  // it, outside the mesh the nearest boundary cell), the tensor-product
+  // Lagrange basis on the Gauss-Lobatto support points there, and the scalar
+  // of V, n or p in physical units, or a quasi Fermi potential from n or p
+  // and V (compute_quasi_fermi_potential, include/solver.h:343-376).
+  __global__ void
+  sample_points_kernel(const SampleArgs A, const double *__restrict__ cell_state,
+                       const double *__restrict__ pts, double *__restrict__ out)
+  {
+    const int NCA = 3 * (A.dim + 1) * A.nb;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.npoints;
+         i += (int64_t)gridDim.x * blockDim.x)
+      {
+        int64_t cell = 0, stride = 1;
+        double  lag[3][4];
+        for (int a = 0; a < A.dim; ++a)
+          {
+            const double rel = (pts[i * 3 + a] - A.origin[a]) / A.h[a];
+            int          ci  = (int)floor(rel);
+            ci               = ci < 0 ? 0 : (ci > A.n[a] - 1 ? A.n[a] - 1 : ci);
+            const double x   = rel - ci;
+            for (int m = 0; m <= A.k; ++m)
+              {
+                double v = 1.;
+                for (int j = 0; j <= A.k; ++j)
+                  if (j != m)
+                    v *= (x - A.gl[j]) / (A.gl[m] - A.gl[j]);
+                lag[a][m] = v;
+              }
+            cell += ci * stride;
+            stride *= A.n[a];
+          }
+        auto scalar = [&](int comp) {
+          const double *cf = cell_state + cell * NCA + (comp * (A.dim + 1) + A.dim) * A.nb;
+          double        s  = 0.;
+          for (int b = 0; b < A.nb; ++b)
+            {
+              double phi = 1.;
+              int    d   = b;
+              for (int a = 0; a < A.dim; ++a)
+                {
+                  phi *= lag[a][d % (A.k + 1)];
+                  d /= (A.k + 1);
+                }
+              s += phi * cf[b];
+            }
+          return s;
+        };
+        double r;
+        if (A.what <= 2)
+          r = scalar(A.what) * (A.what == 0 ? A.V_rescale : A.n_rescale);
+        else
+          {
+            const double V   = scalar(0) * A.V_rescale;
+            const double U_T = A.T * (KB_ / Q_);
+            if (A.what == 3)
+              r = V - A.ec / Q_ - U_T * log(scalar(1) * A.n_rescale / A.nc);
+            else
+              r = V - A.ev / Q_ + U_T * log(scalar(2) * A.n_rescale / A.nv);
+          }
+        out[i] = r;
+      }
+  }
+} // namespace
+
+extern "C" {
+
+int
+ddhdg_sample_points(ddhdg_ctx *c, const double *cell_state, int64_t npoints, const double *points,
+                    int what, double *out, ddhdg_stream_t stream)
+{
+  if (!c || !cell_state || (npoints > 0 && (!points || !out)))
+    return fail(DDHDG_BAD_ARG, "null argument");
+  if (npoints < 0 || what < 0 || what > 4)
+    return fail(DDHDG_BAD_ARG, "what must be 0 (V), 1 (n), 2 (p), 3 (phi_n) or 4 (phi_p)");
+  if (npoints == 0)
+    return DDHDG_OK;
+  SampleArgs A{};
+  A.dim = c->dim;
+  A.k   = c->k;
+  A.nb  = c->nb;
+  for (int a = 0; a < 3; ++a)
+    {
+      A.n[a]      = (a < c->dim) ? c->desc.n[a] : 1;
+      A.origin[a] = c->desc.origin[a];
+      A.h[a]      = (a < c->dim) ? c->desc.h[a] : 1.;
+    }
+  for (int m = 0; m <= c->k && m < 4; ++m)
+    A.gl[m] = c->T.gl[m];
+  A.what      = what;
+  A.V_rescale = c->desc.V_rescale;
+  A.n_rescale = c->desc.n_rescale;
+  A.T         = c->desc.temperature;
+  A.ec        = c->desc.ec_eV * EV_;
+  A.ev        = c->desc.ev_eV * EV_;
+  A.nc        = c->desc.nc;
+  A.nv        = c->desc.nv;
+  A.npoints   = npoints;
+  sample_points_kernel<<<grid_for(c, npoints, 256), 256, 0, (cudaStream_t)stream>>>(A, cell_state, points,
+                                                                                   out);
+  CK(cudaGetLastError());
+  return DDHDG_OK;
+}
+
+int
+ddhdg_local_cell_system(ddhdg_ctx *c, const double *cell_state, const double *trace_state,
+                        int thermo, int64_t ncells, const int64_t *cells, int64_t first_cell,
+                        double *cc, double *ct, double *tc, double *tt, double *cv, double *tv,
+                        ddhdg_stream_t stream)
+{
+  if (!c || !cell_state || !trace_state)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  if (ncells < 0 || (!cells && (first_cell < 0 || first_cell + ncells > c->ncells)))
+    return fail(DDHDG_BAD_ARG, "cell range outside the mesh");
+  if (ncells == 0)
+    return DDHDG_OK;
+  thermo = thermo ? 1 : 0;
+  plain_prepare(c, thermo);
+  KParams P     = make_params(c, thermo);
+  P.cell_state  = cell_state;
+  P.trace_state = trace_state;
+  P.cell0       = first_cell;
+  PlainArgs A{};
+  A.mode  = PlainProbe;
+  A.nlist = ncells;
+  A.cells = cells;
+  A.cc    = cc;
+  A.ct    = ct;
+  A.tc    = tc;
+  A.tt    = tt;
+  A.c     = cv;
+  A.t     = tv;
+  return plain_run(c, thermo, P, A, ncells, (cudaStream_t)stream);
+}
+
+int
+ddhdg_assemble_condense_plain(ddhdg_ctx *c, const double *cell_state, const double *trace_state,
+                              int thermo, double *tt, double *rhs, int32_t *dflag, double *dval,
+                              ddhdg_stream_t stream)
+{
+  if (!c || !cell_state || !trace_state || !tt || !rhs || !dflag || !dval)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo = thermo ? 1 : 0;
+  plain_prepare(c, thermo);
+  KParams P     = make_params(c, thermo);
+  P.cell_state  = cell_state;
+  P.trace_state = trace_state;
+  P.tt          = tt;
+  P.rhs         = rhs;
+  P.dflag       = dflag;
+  P.dval        = dval;
+  PlainArgs A{};
+  A.mode = PlainCondense;
+  return plain_run(c, thermo, P, A, c->ncells, (cudaStream_t)stream);
+}
+
+int
+ddhdg_reconstruct_plain(ddhdg_ctx *c, const double *cell_state, const double *trace_state,
+                        const double *update_trace, double *update_cell, int thermo,
+                        ddhdg_stream_t stream)
+{
+  if (!c || !cell_state || !trace_state || !update_trace || !update_cell)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  thermo = thermo ? 1 : 0;
+  plain_prepare(c, thermo);
+  KParams P     = make_params(c, thermo);
+  P.cell_state  = cell_state;
+  P.trace_state = trace_state;
+  PlainArgs A{};
+  A.mode         = PlainReconstruct;
+  A.update_trace = update_trace;
+  A.update_cell  = update_cell;
+  return plain_run(c, thermo, P, A, c->ncells, (cudaStream_t)stream);
 }
 
 } // extern "C"

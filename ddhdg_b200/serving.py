@@ -120,25 +120,51 @@ class DiodeServer:
 
     max_inflight: requests on the device at once (slots).
     hbm_reserve: bytes of device memory left free for everything else.
-    hbm_limit: treat the device as having at most this many bytes (tests)."""
+    hbm_limit: treat the device as having at most this many bytes (tests).
+    mem_info: callable returning (free, total) device bytes; defaults to
+    cudaMemGetInfo of `device`."""
 
     def __init__(self, max_inflight=8, hbm_reserve=4 << 30, hbm_limit=None, device="cuda:0",
-                 keep_states=False):
+                 keep_states=False, mem_info=None):
         self.max_inflight = max_inflight
         self.hbm_reserve = hbm_reserve
         self.hbm_limit = hbm_limit
         self.device = device
         self.keep_states = keep_states
+        self.mem_info = mem_info
         self.peak_inflight = 0
         self.peak_committed = 0  # largest sum of the in-flight requests' memory estimates
+        self._used_at_start = 0
 
-    def _free_bytes(self, committed):
+    def _mem_info(self):
+        if self.mem_info is not None:
+            return self.mem_info()
         import torch
 
-        free, total = torch.cuda.mem_get_info(self.device)
+        return torch.cuda.mem_get_info(self.device)
+
+    def _start_accounting(self):
+        """Device bytes in use before any request runs (other users of the
+        device, this process's own caches)."""
+        free, total = self._mem_info()
+        self._used_at_start = total - free
+
+    def _free_bytes(self, committed):
+        """Bytes a new request may take.  A request that has been admitted
+        may not have allocated its buffers yet, so the live free figure alone
+        would let a burst of arrivals pass the check against the same memory:
+        the estimates of all requests in flight are subtracted from what was
+        free when the run started, and the live figure only lowers that."""
+        free, total = self._mem_info()
+        cap = total - self._used_at_start
         if self.hbm_limit is not None:
-            free = min(free, self.hbm_limit - committed)
-        return free - self.hbm_reserve
+            cap = min(cap, self.hbm_limit)
+        return min(free, cap - committed) - self.hbm_reserve
+
+    def admissible(self, est, committed):
+        """Whether a request of `est` bytes fits next to `committed` bytes of
+        requests in flight."""
+        return est <= self._free_bytes(committed)
 
     def run(self, requests):
         """Serve the requests (sorted by arrival time); returns their
@@ -153,6 +179,7 @@ class DiodeServer:
         inflight = {}      # rid -> estimated bytes
         committed = [0]
         errors = []
+        self._start_accounting()
         t0 = time.perf_counter()
 
         def worker(req, est, start):
@@ -184,9 +211,9 @@ class DiodeServer:
             est = memory_estimate(req.dim, req.m, req.k)
             with lock:
                 while inflight and (len(inflight) >= self.max_inflight or
-                                    est > self._free_bytes(committed[0])):
+                                    not self.admissible(est, committed[0])):
                     done.wait(timeout=0.05)
-                if not inflight and est > self._free_bytes(committed[0]):
+                if not inflight and not self.admissible(est, committed[0]):
                     errors.append((req.rid, "does not fit in device memory"))
                     i += 1
                     continue

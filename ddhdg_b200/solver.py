@@ -289,6 +289,58 @@ class NPSolver:
                    "reconstruct")
         return out.view(self.ncells, self.Nc_all)
 
+    def get_local_cell_system(self, cells, thermo=False):
+        """get_local_cell_system (src/np_solver.cpp:2337-2445) for a list of
+        cells (indices into the lexicographic cell order): the local system
+        before the Schur complement, assembled on the device.  Returns a dict
+        of arrays with a leading cell axis: cc [Nc][Nc], ct [Nc][Nt],
+        tc [Nt][Nc], tt [Nt][Nt], c [Nc], t [Nt] (Nc: enabled cell dofs)."""
+        torch = _torch()
+        s = self.sizes(thermo)
+        ncomp = 1 if thermo else sum(self.enabled)
+        Nc, Nt = ncomp * (self.dim + 1) * self.nb, s.Nt
+        idx = torch.as_tensor(np.asarray(cells, dtype=np.int64).ravel(), device=self.device)
+        n = int(idx.numel())
+        shapes = dict(cc=(Nc, Nc), ct=(Nc, Nt), tc=(Nt, Nc), tt=(Nt, Nt), c=(Nc,), t=(Nt,))
+        out = {k: torch.empty((n,) + v, dtype=torch.float64, device=self.device) for k, v in shapes.items()}
+        _lib.check(self.L.ddhdg_local_cell_system(self._ctx, self.cell_state.data_ptr(),
+                                                  self.trace_state.data_ptr(), int(thermo), n,
+                                                  idx.data_ptr(), 0,
+                                                  *[out[k].data_ptr() for k in ("cc", "ct", "tc", "tt", "c", "t")],
+                                                  self._sp()), "local_cell_system")
+        return {k: v.cpu().numpy() for k, v in out.items()}
+
+    def assemble_condense_plain(self, thermo=False):
+        """The same outputs as assemble_condense from the plain FP64 device
+        path: the full local systems and an LU of cc per cell, as the
+        reference computes them."""
+        torch = _torch()
+        s = self.sizes(thermo)
+        nc, Nt = self.ncells, s.Nt
+        tt = torch.empty(nc * Nt * Nt, dtype=torch.float64, device=self.device)
+        rhs = torch.empty(nc * Nt, dtype=torch.float64, device=self.device)
+        dflag = torch.empty(nc * Nt, dtype=torch.int32, device=self.device)
+        dval = torch.empty(nc * Nt, dtype=torch.float64, device=self.device)
+        _lib.check(self.L.ddhdg_assemble_condense_plain(self._ctx, self.cell_state.data_ptr(),
+                                                        self.trace_state.data_ptr(), int(thermo),
+                                                        tt.data_ptr(), rhs.data_ptr(), dflag.data_ptr(),
+                                                        dval.data_ptr(), self._sp()), "assemble_condense_plain")
+        return tt.view(nc, Nt, Nt), rhs.view(nc, Nt), dflag.view(nc, Nt), dval.view(nc, Nt)
+
+    def reconstruct_plain(self, update_trace, thermo=False):
+        """The cell update from the plain FP64 device path (cell systems
+        assembled again with the trace update, then solved)."""
+        torch = _torch()
+        ut = update_trace if isinstance(update_trace, torch.Tensor) else \
+            torch.as_tensor(np.ascontiguousarray(update_trace, dtype=np.float64), device=self.device)
+        ut = ut.reshape(-1).contiguous()
+        out = torch.empty(self.ncells * self.Nc_all, dtype=torch.float64, device=self.device)
+        _lib.check(self.L.ddhdg_reconstruct_plain(self._ctx, self.cell_state.data_ptr(),
+                                                  self.trace_state.data_ptr(), ut.data_ptr(),
+                                                  out.data_ptr(), int(thermo), self._sp()),
+                   "reconstruct_plain")
+        return out.view(self.ncells, self.Nc_all)
+
     # ------------------------------------------- global linear system
     def assemble_system(self, thermo=False):
         """assemble_system(false, thermo_eq) + copy_local_to_global
@@ -495,32 +547,22 @@ class NPSolver:
         self.set_state(cs, ts)
 
     def get_solution_on_a_point(self, point, c):
-        """NPSolver::get_solution_on_a_point (src/np_solver.cpp:1637-1700)."""
-        return float(self.evaluate(int(c), np.atleast_2d(point))[0])
+        """NPSolver::get_solution_on_a_point (src/np_solver.cpp:1637-1700):
+        V, n, p (physical units) or the quasi Fermi potential phi_n / phi_p
+        (volts) at one point, evaluated on the device."""
+        return float(self.evaluate(c, np.atleast_2d(point))[0])
 
     def evaluate(self, c, points):
+        """The same at many points [N, dim] (one device launch)."""
+        torch = _torch()
         pts = np.atleast_2d(np.asarray(points, dtype=np.float64))
         if pts.shape[1] < 3:
             pts = np.concatenate([pts, np.zeros((pts.shape[0], 3 - pts.shape[1]))], 1)
-        d = self.dim
-        rel = (pts[:, :d] - np.array(self.origin[:d])) / np.array(self.h[:d])
-        ci = np.clip(np.floor(rel).astype(np.int64), 0, np.array(self.n[:d]) - 1)
-        xi = rel - ci
-        cell = ci[:, 0].copy()
-        if d > 1:
-            cell += self.n[0] * ci[:, 1]
-        if d > 2:
-            cell += self.n[0] * self.n[1] * ci[:, 2]
-        nodes = self.support
-        phi = np.ones((pts.shape[0], self.nb))
-        for a in range(d):
-            V = np.ones((pts.shape[0], self.k + 1))
-            for i in range(self.k + 1):
-                for j in range(self.k + 1):
-                    if i != j:
-                        V[:, i] *= (xi[:, a] - nodes[j]) / (nodes[i] - nodes[j])
-            idx = (np.arange(self.nb) // (self.k + 1) ** a) % (self.k + 1)
-            phi *= V[:, idx]
-        cs = self.get_cell_state()
-        blk = cs[cell, (c * (d + 1) + d) * self.nb:(c * (d + 1) + d + 1) * self.nb]
-        return np.einsum("na,na->n", phi, blk) * self.adim.get_component_rescaling_factor(c)
+        c = Component(c)
+        what = {Component.V: 0, Component.n: 1, Component.p: 2, Component.phi_n: 3, Component.phi_p: 4}[c]
+        dpts = torch.as_tensor(np.ascontiguousarray(pts), device=self.device)
+        out = torch.empty(pts.shape[0], dtype=torch.float64, device=self.device)
+        _lib.check(self.L.ddhdg_sample_points(self._ctx, self.cell_state.data_ptr(), pts.shape[0],
+                                              dpts.data_ptr(), what, out.data_ptr(), self._sp()),
+                   "sample_points")
+        return out.cpu().numpy()

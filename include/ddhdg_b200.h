@@ -176,6 +176,43 @@ int ddhdg_assemble_condense_noalloc(ddhdg_ctx *ctx, const double *cell_state,
                                     double *tt, double *rhs, int32_t *dflag,
                                     double *dval, ddhdg_stream_t stream);
 
+/* get_local_cell_system(level, index, thermo_eq) (src/np_solver.cpp:
+ * 2337-2445), the per-cell parity probe: the local system of each listed cell
+ * as the reference's per-cell worker leaves it before the Schur complement
+ * (include/assembling_methods.template.h:2290-2647 with the Dirichlet columns
+ * of ct folded into cc_rhs, src/local_condenser.cpp:142-160), assembled on the
+ * device term by term.  Nc = ncomp * (dim + 1) * (k + 1)^dim enabled cell
+ * dofs in the FESystem order restricted to the enabled components, Nt as in
+ * ddhdg_get_sizes.  Cells: the device list cells[ncells], or, with cells ==
+ * NULL, the range [first_cell, first_cell + ncells).  Outputs (device, any
+ * may be NULL), per listed cell in list order:
+ *   cc [Nc][Nc], ct [Nc][Nt], tc [Nt][Nc], tt [Nt][Nt], c [Nc], t [Nt]. */
+int ddhdg_local_cell_system(ddhdg_ctx *ctx, const double *cell_state,
+                            const double *trace_state, int thermo_eq,
+                            int64_t ncells, const int64_t *cells,
+                            int64_t first_cell, double *cc, double *ct,
+                            double *tc, double *tt, double *c, double *t,
+                            ddhdg_stream_t stream);
+
+/* The reference's per-cell algorithm as written, on the device (FP64): the
+ * full local system of every cell assembled term by term
+ * (include/assembling_methods.template.h:134-2160), Dirichlet columns folded
+ * (src/local_condenser.cpp:142-160), then the Schur complement through an LU
+ * factorisation of the row-equilibrated cc with partial pivoting (in place of
+ * cc.gauss_jordan(), T:2651-2686).  Same outputs as ddhdg_assemble_condense;
+ * it keeps no reconstruction data: ddhdg_reconstruct_plain assembles the
+ * cell systems again with the trace update and solves them (T:2688-2697),
+ * as the reference's second assemble_system pass does.  This is the plain
+ * FP64 GPU path that the block-eliminated kernels are measured against. */
+int ddhdg_assemble_condense_plain(ddhdg_ctx *ctx, const double *cell_state,
+                                  const double *trace_state, int thermo_eq,
+                                  double *tt, double *rhs, int32_t *dflag,
+                                  double *dval, ddhdg_stream_t stream);
+int ddhdg_reconstruct_plain(ddhdg_ctx *ctx, const double *cell_state,
+                            const double *trace_state,
+                            const double *update_trace, double *update_cell,
+                            int thermo_eq, ddhdg_stream_t stream);
+
 /* copy_local_to_global (src/np_solver.cpp:1293-1322): scatter the per-cell
  * condensed systems into the global CSR trace matrix (values[nnz], rows and
  * columns from ddhdg_get_csr) and rhs[n_trace_dofs]; Dirichlet rows become
@@ -275,6 +312,16 @@ int ddhdg_project_trace(ddhdg_ctx *ctx, const double *vals_face, int comp,
 int ddhdg_project_density(ddhdg_ctx *ctx, int comp, double qf,
                           double *cell_state, double *trace_state,
                           ddhdg_stream_t stream);
+
+/* get_solution_on_a_point (src/np_solver.cpp:1637-1700) for npoints points
+ * [npoints][3] (mesh units, device): what = 0, 1, 2 gives V (volts), n, p
+ * (m^-3) of the cell field; 3, 4 the quasi Fermi potentials phi_n, phi_p
+ * (volts, include/solver.h:343-376).  The cell of a point on an interior face
+ * is the one above it along each axis; points outside the mesh use the
+ * nearest boundary cell.  out [npoints] on the device. */
+int ddhdg_sample_points(ddhdg_ctx *ctx, const double *cell_state,
+                        int64_t npoints, const double *points, int what,
+                        double *out, ddhdg_stream_t stream);
 
 /* Reference coordinates in [0,1]^dim of the quadrature points and support
  * points the kernels use for a (dim, degree) pair, so that callers evaluate

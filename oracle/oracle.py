@@ -378,13 +378,27 @@ class OracleSolver:
                                        _dp(cc), _dp(ct), _dp(tc), _dp(tt), _dp(crhs), _dp(trhs))
         return dict(cc=cc, ct=ct, tc=tc, tt=tt, c=crhs, t=trhs)
 
-    def local_cell_systems(self, thermo=False, update_trace=None):
-        """Local systems (cc, ct, tc, tt, cc_rhs, tt_rhs) of every cell, as
-        assembled term by term before the Schur complement."""
+    def local_cell_systems(self, thermo=False, update_trace=None, cells=None):
+        """Local systems (cc, ct, tc, tt, cc_rhs, tt_rhs) of every cell (or of
+        the listed `cells`, in that order), as assembled term by term before
+        the Schur complement."""
         P = self._struct(thermo=thermo)
         sizes = np.zeros(9, dtype=np.int32)
         lib().oracle_sizes(ctypes.byref(P), _ip(sizes))
         Nc, Nt, n = int(sizes[1]), int(sizes[2]), self.ncells
+        if cells is not None:
+            assert update_trace is None
+            cells = np.asarray(cells, dtype=np.int64)
+            out = [np.zeros((len(cells),) + s) for s in ((Nc, Nc), (Nc, Nt), (Nt, Nc), (Nt, Nt), (Nc,), (Nt,))]
+            cs = np.ascontiguousarray(self.cell_state)
+            ts = np.ascontiguousarray(self.trace_state)
+            for i, cell in enumerate(cells):
+                bufs = [np.zeros(a.shape[1:]) for a in out]
+                lib().oracle_local_cell_system(ctypes.byref(P), _dp(cs), _dp(ts), int(cell), int(thermo),
+                                               *[_dp(b) for b in bufs])
+                for a, b in zip(out, bufs):
+                    a[i] = b
+            return tuple(out)
         cc = np.zeros((n, Nc, Nc))
         ct = np.zeros((n, Nc, Nt))
         tc = np.zeros((n, Nt, Nc))
@@ -399,32 +413,93 @@ class OracleSolver:
                                         _dp(tc), _dp(tt), _dp(cr), _dp(tr), self.nthreads)
         return cc, ct, tc, tt, cr, tr
 
+    @staticmethod
+    def _refined_solve(A, B, sweeps=3):
+        """Row-equilibrated LU solve of the batched systems A X = B, followed
+        by iterative refinement with residuals in long double: the result is
+        the FP64 rounding of the exact solution even where the cell system is
+        ill-conditioned (3D Dirichlet cells), so it serves as the parity
+        target of any FP64 implementation."""
+        d = 1.0 / np.abs(A).max(2, keepdims=True)
+        Ad, Bd = A * d, B * d
+        X = np.linalg.solve(Ad, Bd)
+        Al, Bl, Xl = Ad.astype(np.longdouble), Bd.astype(np.longdouble), X.astype(np.longdouble)
+        for _ in range(sweeps):
+            R = (Bl - Al @ Xl).astype(np.float64)
+            Xl = Xl + np.linalg.solve(Ad, R)
+        return Xl
+
     def reconstruct_accurate(self, update_trace, thermo=False):
-        """Reconstruction-pass local systems solved with a row-equilibrated LU."""
+        """Reconstruction-pass local systems solved accurately (row-
+        equilibrated LU refined with long-double residuals)."""
         cc, _, _, _, cr, _ = self.local_cell_systems(thermo, update_trace)
-        d = 1.0 / np.abs(cc).max(2, keepdims=True)
-        x = np.linalg.solve(cc * d, (cr * d[:, :, 0])[:, :, None])[:, :, 0]
-        P = self._struct(thermo=thermo)
+        cr0 = self.local_cell_systems(thermo)[4]
+        x = self._refined_solve(cc, cr[:, :, None])[:, :, 0].astype(np.float64)
+        # magnitude of the summed terms through the local solve: |cc^-1| times
+        # (|residual part| + |trace-update part|) of the right-hand side
+        mag = (np.abs(np.linalg.inv(cc)) @ (np.abs(cr0) + np.abs(cr - cr0))[:, :, None])[:, :, 0]
         out = np.zeros((self.ncells, self.Nc_all))
+        sc = np.zeros((self.ncells, self.Nc_all))
         en = [True, False, False] if thermo else self.enabled
         idx = [i for i in range(self.Nc_all) if en[i // ((self.dim + 1) * self.nb)]]
         out[:, idx] = x
+        sc[:, idx] = mag
+        # [3 components][flux, scalar] magnitude of the summed terms
+        d, nb = self.dim, self.nb
+        blk = sc.reshape(self.ncells, 3, d + 1, nb)
+        self.reconstruct_block_scale = np.stack([np.abs(blk[:, :, :d]).max((0, 2, 3)),
+                                                 np.abs(blk[:, :, d]).max((0, 2))], 1)
         return out
 
-    def condense_accurate(self, thermo=False):
+    def condense_accurate(self, thermo=False, cells=None):
         """Schur complement tt + tc cc^-1 [ct | cc_rhs] of the term-by-term
-        local systems with a row-equilibrated LU solve (numpy), used to
-        separate round-off of the reference's inversion from assembly."""
-        cc, ct, tc, tt, cr, tr = self.local_cell_systems(thermo)
-        d = 1.0 / np.abs(cc).max(2, keepdims=True)
+        local systems, with cc^-1 applied by a row-equilibrated LU refined in
+        long double (so the result does not carry the round-off of any one
+        inversion) and the products summed in long double.  Used to separate
+        round-off of the reference's inversion from assembly, and as the
+        parity target.  `cells` restricts it to a subset (in that order).
+
+        Sets ``condense_term_scale`` (global magnitudes of the summed terms of
+        tt and rhs), ``condense_block_scale`` = (tt [ncomp][ncomp],
+        rhs [ncomp]): the magnitude of the summed terms (tt or tt_rhs and the
+        Schur product) inside each (row component, column component) block of
+        the restricted trace order [face][component][node], and
+        ``condense_solve_scale``, the same with the terms summed inside the
+        local solve counted too (|tt| + |tc| |cc^-1| |ct|, |tr| + |tc| |cc^-1|
+        |cc_rhs|)."""
+        cc, ct, tc, tt, cr, tr = self.local_cell_systems(thermo, cells=cells)
         rhs = np.concatenate([cr[:, :, None], ct], 2)
-        X = np.linalg.solve(cc * d, rhs * d)
-        tcX = tc @ X
-        S = tt + tcX[:, :, 1:]
-        g = tr + tcX[:, :, 0]
+        Xl = self._refined_solve(cc, rhs)
+        tcXl = tc.astype(np.longdouble) @ Xl
+        tcX = tcXl.astype(np.float64)
+        S = (tt + tcXl[:, :, 1:]).astype(np.float64)
+        g = (tr + tcXl[:, :, 0]).astype(np.float64)
         # magnitude of the summed terms (round-off scale of S and g)
         self.condense_term_scale = (max(np.abs(tt).max(), np.abs(tcX[:, :, 1:]).max()),
                                     max(np.abs(tr).max(), np.abs(tcX[:, :, 0]).max()))
+        ncomp = len(self.enabled_list(thermo))
+        comp = (np.arange(tt.shape[1]) // self.nf) % ncomp
+        # magnitudes through the local solve as well: |tt| + |tc| |cc^-1| |ct|
+        # and |tr| + |tc| |cc^-1| |cc_rhs| (the componentwise bound of any
+        # backward-stable solve; in 3D Dirichlet cells cc^-1 cc_rhs is a
+        # cancellation of terms 1e6 times larger than the result)
+        aTC = np.abs(tc) @ np.abs(np.linalg.inv(cc))
+        s3t = np.abs(tt) + aTC @ np.abs(ct)
+        s3r = np.abs(tr) + (aTC @ np.abs(cr)[:, :, None])[:, :, 0]
+        bt = np.zeros((ncomp, ncomp))
+        br = np.zeros(ncomp)
+        st = np.zeros((ncomp, ncomp))
+        sr = np.zeros(ncomp)
+        for a in range(ncomp):
+            ra = comp == a
+            br[a] = max(np.abs(tr[:, ra]).max(), np.abs(tcX[:, ra, 0]).max())
+            sr[a] = s3r[:, ra].max()
+            for b in range(ncomp):
+                cb = np.flatnonzero(comp == b) + 1
+                bt[a, b] = max(np.abs(tt[:, ra][:, :, cb - 1]).max(), np.abs(tcX[:, ra][:, :, cb]).max())
+                st[a, b] = s3t[:, ra][:, :, cb - 1].max()
+        self.condense_block_scale = (bt, br)
+        self.condense_solve_scale = (st, sr)
         return S, g
 
     def assemble_condense(self, thermo=False):

@@ -51,10 +51,16 @@ def compute(name):
     _, _, flag, val = o.assemble_condense()
     tt, rhs = o.condense_accurate()
     s_tt, s_rhs = o.condense_term_scale
+    b_tt, _ = o.condense_block_scale
+    _, b_rhs = o.condense_solve_scale
     rng = np.random.default_rng(seed + 100)
     upd = 1e-3 * rng.standard_normal((o.nfaces, 3, o.nf)) * max(np.abs(o.trace_state).max(), 1e-3)
     du = o.reconstruct_accurate(upd)
+    # per-block magnitudes of the summed terms: tt [comp][comp] (tt and the
+    # Schur product), rhs [comp] (through the local solve), cell update
+    # [comp][flux, scalar]
     return dict(cell=cell, trace=trace, tt=tt, rhs=rhs, dflag=flag, dval=val, s_tt=s_tt, s_rhs=s_rhs,
+                b_tt=b_tt, b_rhs=b_rhs, b_du=o.reconstruct_block_scale,
                 update_trace=upd, update_cell=du)
 
 

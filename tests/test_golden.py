@@ -16,6 +16,6 @@ def test_oracle_reproduces_fixture(name):
     ref = np.load(os.path.join(HERE, name + ".npz"))
     got = mg.compute(name)
     assert np.array_equal(got["dflag"], ref["dflag"])
-    for key in ("cell", "trace", "tt", "rhs", "dval", "update_cell"):
+    for key in ("cell", "trace", "tt", "rhs", "dval", "update_cell", "b_tt", "b_rhs", "b_du"):
         scale = max(np.abs(ref[key]).max(), 1e-300)
         assert np.abs(got[key] - ref[key]).max() <= 1e-12 * scale, key

@@ -4,12 +4,30 @@
 * the nested-dissection trace solve satisfies the assembled system
   (A x - b from the per-cell blocks, on the device, to FP64 round-off);
 * a forward-biased Newton solve (warm start from equilibrium) drives the
-  assembled residual down by at least eight orders of magnitude."""
+  assembled residual down by at least eight orders of magnitude;
+* at the converged state, the condensed systems of a seeded sample of 1 280
+  cells (both junction columns, both contacts, the other boundaries and the
+  interior) match the oracle's to 1e-10 in every component block."""
 
 import numpy as np
 import pytest
 
 from ddhdg_b200 import workloads
+from tests.gpu_helpers import block_rel_errs
+
+
+def _sample_cells(m, n_interior=1024, seed=7):
+    """Cells of an m x m mesh (x fastest): the two columns at the junction,
+    the two contact columns, the bottom and top rows, and seeded interior
+    cells."""
+    ix = np.arange(m * m) % m
+    iy = np.arange(m * m) // m
+    special = np.flatnonzero((ix == m // 2 - 1) | (ix == m // 2) | (ix == 0) | (ix == m - 1) |
+                             (iy == 0) | (iy == m - 1))
+    rng = np.random.default_rng(seed)
+    special = rng.choice(special, size=min(256, special.size), replace=False)
+    rest = np.setdiff1d(np.arange(m * m), special)
+    return np.sort(np.concatenate([special, rng.choice(rest, size=n_interior, replace=False)]))
 
 pytestmark = pytest.mark.gpu
 
@@ -65,6 +83,21 @@ def test_full_size_solve_and_newton():
     g.assemble_system()
     r1 = float(g._system["rhs"].abs().max())
     assert r1 <= 1e-8 * r0, (r0, r1)
+    # 3) the condensed systems at the converged state against the oracle, on
+    # a sample of cells
+    from oracle.oracle import OracleSolver
+
+    tt, rhs, flag, _ = g.assemble_condense()
+    o = OracleSolver(pb, prm, adim)
+    o.cell_state[:] = g.get_cell_state()
+    o.trace_state[:] = g.get_trace_state()
+    sel = _sample_cells(256)
+    assert sel.size >= 1024
+    S, gv = o.condense_accurate(cells=sel)
+    e_tt, e_rhs, table = block_rel_errs(tt.cpu().numpy()[sel], rhs.cpu().numpy()[sel], S, gv, o)
+    print(f"256x256 k=2 sample of {sel.size} cells: worst block tt {e_tt:.2e}, rhs {e_rhs:.2e}")
+    assert e_tt < 1e-10, table
+    assert e_rhs < 1e-10, table
 
 
 def test_full_size_mixed_newton_matches_fp64():

@@ -40,13 +40,17 @@ def test_residual_jacobian_and_solution_match_oracle(dim, m, k):
     idx = np.arange(n).reshape(o.nfaces, 3, o.nf)
     comps = {Component(c): idx[:, c, :].ravel() for c in range(3)}
     assert set(J) == {(c1, c2) for c1 in comps for c2 in comps}
+    # each (component, component) block at the scale of the terms summed in
+    # that block (a global entry sums at most two cells' contributions)
+    b_tt, b_rhs = o.condense_block_scale
     for (c1, c2), blk in J.items():
         ref = A[comps[c1]][:, comps[c2]].toarray()
-        err = np.abs(blk.toarray() - ref).max() / max(np.abs(ref).max(), s_tt)
+        err = np.abs(blk.toarray() - ref).max() / max(2 * b_tt[int(c1), int(c2)], 1e-300)
         assert err < TOL, (c1, c2, err)
     for c, v in r.items():
         ref = b[comps[c]]
-        err = np.abs(v - ref).max() / max(np.abs(ref).max(), s_rhs)
+        # Dirichlet rows carry the projected values (trace scale)
+        err = np.abs(v - ref).max() / max(2 * b_rhs[int(c)], np.abs(o.trace_state[:, int(c)]).max())
         assert err < TOL, (c, err)
     # the solution of the assembled system: against a sparse LU of the same
     # (device-assembled) system, and, within its conditioning, the oracle's

@@ -129,3 +129,40 @@ def test_diode_forward_bias_newton_iterates_match_oracle():
         g.private_run(0.0, 0.0, it)
         ref_cell, ref_trace = hist[it - 1]
         assert _field_rel_err(g.get_cell_state(), ref_cell, g.get_trace_state(), ref_trace, o) < 1e-10, it
+
+
+def test_config1_reference_jacobian_iterates_match_oracle():
+    """The drop-in as written: BASELINE's first diode (32x32 quads, degree 1,
+    zero bias, from thermodynamic equilibrium) with the reference's own
+    Jacobian (no consistency switches; src/np_solver.cpp:1452-1561 with
+    include/assembling_methods.template.h:484-527).  That iteration diverges
+    (the updates grow ~10-100x per step, on the CPU as well), so the iterates
+    are compared, not a converged result: after 1, 2 and 3 undamped steps
+    the GPU state matches the oracle's per component block (V, n, p; cell
+    and trace coefficients).  The growth of the iterates also amplifies the
+    difference of round-off between the two implementations; the bound for
+    step s is 1e-10 times the growth of the update norm up to that step."""
+    NPSolver = _npsolver()
+    pb, prm, adim = cases.diode(dim=2, m=32, k=1)
+    assert not prm.consistent_drift_jacobian and not prm.consistent_recombination_jacobian
+    o = O.OracleSolver(pb, prm, adim)
+    o.compute_local_charge_neutrality()
+    o.private_run(1e-10, 1e-10, 50, thermo=True)
+    o.project_quasi_fermi(1)
+    o.project_quasi_fermi(2)
+    start_cell, start_trace = o.cell_state.copy(), o.trace_state.copy()
+    o.private_run(0.0, 0.0, 3, record=True)
+    hist = o.newton_history
+    g = NPSolver(pb, prm, adim)
+    growth = 1.0
+    prev = np.abs(start_cell).max()
+    for it in (1, 2, 3):
+        g.set_state(start_cell, start_trace)
+        g.private_run(0.0, 0.0, it)
+        ref_cell, ref_trace = hist[it - 1]
+        cur = np.abs(ref_cell).max()
+        growth *= max(cur / prev, 1.0)
+        prev = cur
+        e = _field_rel_err(g.get_cell_state(), ref_cell, g.get_trace_state(), ref_trace, o)
+        print(f"reference Jacobian, step {it}: field error {e:.2e} (bound {1e-10 * growth:.1e})")
+        assert e < 1e-10 * growth, (it, e)

@@ -2,12 +2,18 @@
 algorithm restated), through the C ABI.
 
 The condensed systems are compared with the oracle's term-by-term local
-matrices condensed by a row-equilibrated LU.  The tolerance 1e-10 is relative
-to the magnitude of the terms that are summed: in the junction cells of the
-diodes the condensed right-hand side is a difference of two terms up to 5e6
-times larger than itself, so FP64 round-off of any implementation is relative
-to those terms, not to the result.  The oracle's own reference-style inversion
-is pinned against the same quantity separately."""
+matrices condensed by a row-equilibrated LU refined in long double.  The
+tolerance 1e-10 holds in every (row component, column component) block of tt
+and every component block of rhs separately, relative to the magnitude of the
+terms summed inside that block: in the junction cells of the diodes the
+condensed right-hand side is a difference of two terms up to 5e6 times larger
+than itself, so FP64 round-off of any implementation is relative to those
+terms, not to the result; and the p-n coupling block is ~1e-4 of the V-n one,
+so a global scale would not check it.  The reconstructed cell update is
+checked the same way per component and per field (flux, scalar).  The
+oracle's own reference-style (unequilibrated Gauss-Jordan) inversion is
+pinned against the same target on the global scale only: in 3D Dirichlet
+cells its round-off reaches 2e-8 of the V block."""
 
 import numpy as np
 import pytest
@@ -16,7 +22,7 @@ from ddhdg_b200.problem import (CellFaceTauNPSolverParameters, Component, DDFlux
                                 LinearRecombinationTerm, NonlinearSolverParameters,
                                 FixedTauNPSolverParameters, BoundaryConditionType as BCT)
 from tests import cases
-from tests.gpu_helpers import make_pair, rel_err
+from tests.gpu_helpers import block_rel_errs, cell_block_rel_err, make_pair, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -33,10 +39,9 @@ def compare_condense(g, o, thermo=False, tol=TOL):
     # match it to FP64 round-off
     S, g_ = o.condense_accurate(thermo)
     s_tt, s_rhs = o.condense_term_scale
-    e_tt = rel_err(tt.cpu().numpy(), S, floor=s_tt)
-    e_rhs = rel_err(rhs.cpu().numpy(), g_, floor=s_rhs)
-    assert e_tt < tol, e_tt
-    assert e_rhs < tol, e_rhs
+    e_tt, e_rhs, table = block_rel_errs(tt.cpu().numpy(), rhs.cpu().numpy(), S, g_, o, thermo)
+    assert e_tt < tol, table
+    assert e_rhs < tol, table
     # the reference's own inversion (LU of the transpose, FullMatrix::
     # gauss_jordan) agrees with it within its round-off
     assert rel_err(ott, S, floor=s_tt) < tol
@@ -54,8 +59,8 @@ def compare_reconstruct(g, o, thermo=False, tol=TOL, seed=5):
     gu = g.reconstruct(upd, thermo).cpu().numpy()
     ou = o.reconstruct(upd, thermo)
     acc = o.reconstruct_accurate(upd, thermo)
-    e = rel_err(gu, acc)
-    assert e < tol, e
+    e, table = cell_block_rel_err(gu, acc, o)
+    assert e < tol, table
     assert rel_err(ou, acc) < 1e-5
 
 

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from ddhdg_b200 import _lib
-from ddhdg_b200.problem import DDFluxType
+from ddhdg_b200.problem import DDFluxType, Precision
 from tests import cases
 from tests.gpu_helpers import make_pair
 
@@ -35,15 +35,22 @@ def _noalloc(g, thermo, outs):
 CELL, QS = DDFluxType.use_cell, DDFluxType.qiu_shi_stabilization
 
 
+FP64, MIXED = Precision.fp64, Precision.mixed
+
+
 # 3D k = 2 with the drift columns keeps R outside shared memory, so both
-# parts of the scratch are exercised
-@pytest.mark.parametrize("dim,m,k,flux", [(2, 8, 2, CELL), (2, 6, 1, QS), (3, 2, 2, QS),
-                                          (2, 4, 3, CELL), (1, 8, 2, CELL)])
-def test_noalloc_matches_assemble_condense_twice(dim, m, k, flux):
+# parts of the scratch are exercised; a mixed-precision context must run the
+# same FP32-Jacobian kernel as ddhdg_assemble_condense
+@pytest.mark.parametrize("dim,m,k,flux,prec", [(2, 8, 2, CELL, FP64), (2, 6, 1, QS, FP64),
+                                               (3, 2, 2, QS, FP64), (2, 4, 3, CELL, FP64),
+                                               (1, 8, 2, CELL, FP64), (2, 8, 2, CELL, MIXED),
+                                               (3, 3, 1, QS, MIXED)])
+def test_noalloc_matches_assemble_condense_twice(dim, m, k, flux, prec):
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("needs a GPU")
     pb, prm, adim = cases.diode(dim=dim, m=m, k=k, flux=flux)
+    prm.precision = prec
     g, _ = make_pair(pb, prm, adim)
     for thermo in (False, True):
         ref = [t.reshape(-1).cpu().numpy() for t in g.assemble_condense(thermo)]
@@ -80,3 +87,23 @@ def test_noalloc_rejects_problems_beyond_its_scratch():
     assert code == 1, code  # DDHDG_BAD_ARG
     msg = g.L.ddhdg_last_error().decode()
     assert "bytes of condensation scratch" in msg and str(NOALLOC_BYTES) in msg, msg
+
+
+def test_noalloc_warm_calls_leave_device_memory_unchanged():
+    """The point of the entry point: after a first call (which may load the
+    kernel's module), further calls take no device memory at all."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    pb, prm, adim = cases.diode(dim=2, m=8, k=2)
+    g, _ = make_pair(pb, prm, adim)
+    nc, Nt = g.ncells, g.sizes(False).Nt
+    outs = _outputs(torch, nc, Nt, g.device)
+    _lib.check(_noalloc(g, False, outs), "assemble_condense_noalloc")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(g.device)
+    for _ in range(3):
+        _lib.check(_noalloc(g, False, outs), "assemble_condense_noalloc")
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(g.device)
+    assert free1 == free0, (free0, free1)
