@@ -29,7 +29,9 @@ EXPORTS = [
     "ddhdg_reference_points", "ddhdg_last_error", "ddhdg_assemble_condense_noalloc",
     "ddhdg_solve_condensed", "ddhdg_assemble_condense_host", "ddhdg_reconstruct_host",
     "ddhdg_set_solver_graphs", "ddhdg_local_cell_system", "ddhdg_assemble_condense_plain",
-    "ddhdg_reconstruct_plain", "ddhdg_sample_points",
+    "ddhdg_reconstruct_plain", "ddhdg_sample_points", "ddhdg_batch_create", "ddhdg_batch_destroy",
+    "ddhdg_batch_condense", "ddhdg_batch_reconstruct", "ddhdg_batch_set_shape", "ddhdg_batch_get_shape",
+    "ddhdg_batch_autotune",
 ]
 
 
@@ -55,6 +57,14 @@ class Sizes(ctypes.Structure):
         ("ncells", c_int64), ("nfaces", c_int64), ("Nc_all", c_int), ("Nt", c_int),
         ("ncomp", c_int), ("nqc", c_int), ("nqf", c_int), ("nb", c_int), ("nf", c_int),
         ("n_trace_dofs", c_int64), ("nnz", c_int64),
+    ]
+
+
+class BatchItem(ctypes.Structure):
+    _fields_ = [
+        ("ctx", c_void_p), ("cell_state", c_void_p), ("trace_state", c_void_p),
+        ("tt", c_void_p), ("rhs", c_void_p), ("dflag", c_void_p), ("dval", c_void_p),
+        ("update_trace", c_void_p), ("update_cell", c_void_p),
     ]
 
 
@@ -101,6 +111,13 @@ def load(build_if_missing: bool = True):
     L.ddhdg_assemble_condense_plain.argtypes = L.ddhdg_assemble_condense.argtypes
     L.ddhdg_reconstruct_plain.argtypes = L.ddhdg_reconstruct.argtypes
     L.ddhdg_sample_points.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_int, c_void_p, c_void_p]
+    L.ddhdg_batch_create.argtypes = [P(BatchItem), c_int, c_int, P(c_void_p)]
+    L.ddhdg_batch_destroy.argtypes = [c_void_p]
+    L.ddhdg_batch_condense.argtypes = [c_void_p, c_void_p]
+    L.ddhdg_batch_reconstruct.argtypes = [c_void_p, c_void_p]
+    L.ddhdg_batch_set_shape.argtypes = [c_void_p, P(c_int), c_int]
+    L.ddhdg_batch_get_shape.argtypes = [c_void_p, P(c_int), P(c_int), P(c_int), P(c_int)]
+    L.ddhdg_batch_autotune.argtypes = [c_void_p, c_int, P(ctypes.c_float), c_void_p]
     L.ddhdg_newton.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, c_int,
                                c_double, P(c_int), P(c_double), c_void_p]
     L.ddhdg_last_timings.argtypes = [c_void_p, P(c_double), P(c_double), P(c_double), P(c_int)]

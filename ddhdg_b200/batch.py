@@ -1,0 +1,105 @@
+"""Batched condensation: many devices (diodes) of different mesh sizes and
+polynomial degrees condensed in ONE persistent launch per Newton step, and
+reconstructed in one more (``ddhdg_batch_*`` of the C ABI).
+
+The reference condenses one device at a time, its per-cell worker run over
+that device's cells by WorkStream (include/assembling_methods.template.h:
+67-88).  ``CondenseBatch`` hands a work list of tiles (device, range of its
+cells) to the CTAs of one grid; the tile sizes per degree and the CTAs per SM
+come from ``autotune()``, which times the batch's own launch.  Every device's
+outputs are bitwise those of its own ``NPSolver.assemble_condense`` /
+``reconstruct``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+from . import _lib
+
+
+class CondenseBatch:
+    """One launch per Newton step over the contexts of `solvers`
+    (``NPSolver`` objects of one dimension, FP64).  The outputs of solver i
+    are ``tt[i]``, ``rhs[i]``, ``dflag[i]``, ``dval[i]`` (shaped like
+    ``NPSolver.assemble_condense``); the reconstruction reads
+    ``update_trace[i]`` ([nfaces * 3 * nf]) and writes ``update_cell[i]``.
+    The solvers' state tensors must stay in place (the launches are replayed
+    from CUDA graphs)."""
+
+    def __init__(self, solvers, thermo=False):
+        import torch
+
+        self.solvers = list(solvers)
+        self.thermo = bool(thermo)
+        self.L = _lib.load()
+        dev = self.solvers[0].device
+        self.tt, self.rhs, self.dflag, self.dval = [], [], [], []
+        self.update_trace, self.update_cell = [], []
+        items = (_lib.BatchItem * len(self.solvers))()
+        for i, g in enumerate(self.solvers):
+            s = g.sizes(thermo)
+            nc, Nt = g.ncells, s.Nt
+            self.tt.append(torch.empty((nc, Nt, Nt), dtype=torch.float64, device=dev))
+            self.rhs.append(torch.empty((nc, Nt), dtype=torch.float64, device=dev))
+            self.dflag.append(torch.empty((nc, Nt), dtype=torch.int32, device=dev))
+            self.dval.append(torch.empty((nc, Nt), dtype=torch.float64, device=dev))
+            self.update_trace.append(torch.zeros(g.nfaces * 3 * g.nf, dtype=torch.float64, device=dev))
+            self.update_cell.append(torch.empty((nc, g.Nc_all), dtype=torch.float64, device=dev))
+            it = items[i]
+            it.ctx = g._ctx
+            it.cell_state = g.cell_state.data_ptr()
+            it.trace_state = g.trace_state.data_ptr()
+            it.tt = self.tt[i].data_ptr()
+            it.rhs = self.rhs[i].data_ptr()
+            it.dflag = self.dflag[i].data_ptr()
+            it.dval = self.dval[i].data_ptr()
+            it.update_trace = self.update_trace[i].data_ptr()
+            it.update_cell = self.update_cell[i].data_ptr()
+        self._items = items
+        self._b = ctypes.c_void_p()
+        _lib.check(self.L.ddhdg_batch_create(items, len(self.solvers), int(self.thermo), ctypes.byref(self._b)),
+                   "batch_create")
+        self.stream = self.solvers[0].stream
+        self.cells = sum(g.ncells for g in self.solvers)
+
+    def _sp(self):
+        return ctypes.c_void_p(self.stream.cuda_stream)
+
+    def condense(self):
+        _lib.check(self.L.ddhdg_batch_condense(self._b, self._sp()), "batch_condense")
+
+    def reconstruct(self):
+        _lib.check(self.L.ddhdg_batch_reconstruct(self._b, self._sp()), "batch_reconstruct")
+
+    def autotune(self, reps=3):
+        """Pick the cells per tile of every degree and the CTAs per SM by
+        timing this batch's condensation launch; returns the best time (ms)."""
+        ms = ctypes.c_float()
+        _lib.check(self.L.ddhdg_batch_autotune(self._b, int(reps), ctypes.byref(ms), self._sp()),
+                   "batch_autotune")
+        return float(ms.value)
+
+    def shape(self):
+        cpt = (ctypes.c_int * 3)()
+        cps, grid, nt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self.L.ddhdg_batch_get_shape(self._b, cpt, ctypes.byref(cps), ctypes.byref(grid),
+                                                ctypes.byref(nt)), "batch_get_shape")
+        return {"cells_per_tile": {1: cpt[0], 2: cpt[1], 3: cpt[2]}, "ctas_per_sm": cps.value,
+                "grid": grid.value, "tiles": nt.value}
+
+    def set_shape(self, cells_per_tile, ctas_per_sm):
+        """cells_per_tile: {degree: cells} for degrees 1..3."""
+        cpt = (ctypes.c_int * 3)(*[int(cells_per_tile[k]) for k in (1, 2, 3)])
+        _lib.check(self.L.ddhdg_batch_set_shape(self._b, cpt, int(ctas_per_sm)), "batch_set_shape")
+
+    def close(self):
+        if self._b:
+            self.L.ddhdg_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/ddhdg_b200.h"
+#include "hdg_batch.cuh"
 #include "hdg_condense.cuh"
 #include "hdg_condense3.cuh"
 #include "hdg_kernels.cuh"
@@ -129,6 +130,7 @@ struct ddhdg_ctx
   int                face_ext[3][3] = {{1, 1, 1}, {1, 1, 1}, {1, 1, 1}};
   int                enabled[3]     = {1, 1, 1};
   Tables             T;
+  Tables             Tu; // the same tables on the unit cell (constant-bank copies)
   TabOff             to{};
   DevBuf<double>     tables, doping, rec_a, rec_b, rec_c, tau_table, bc_val;
   DevBuf<int32_t>    bc;
@@ -452,6 +454,8 @@ namespace
           P.face_ext[a][b] = c->face_ext[a][b];
       }
     P.ncells      = c->ncells;
+    for (int a = 0; a < 3; ++a)
+      P.ih[a] = (a < c->dim) ? 1. / d.h[a] : 1.;
     P.tables      = c->tables.p;
     P.to          = c->to;
     P.eps         = d.eps;
@@ -1018,6 +1022,10 @@ ddhdg_ctx_create(const ddhdg_problem_desc *d, ddhdg_ctx **out)
   c->dim  = d->dim;
   c->k    = d->degree;
   c->T    = build_tables(d->dim, d->degree, d->h);
+  {
+    const double unit[3] = {1., 1., 1.};
+    c->Tu                = build_tables(d->dim, d->degree, unit);
+  }
   c->nb   = c->T.nb;
   c->nf   = c->T.nf;
   c->nqc  = c->T.nqc;
@@ -1269,7 +1277,7 @@ condense_range(ddhdg_ctx *c, const double *cell_state, const double *trace_state
   if (per_sm < 1)
     return fail(DDHDG_BAD_ARG, "condense kernel does not fit on an SM");
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(units, (int64_t)per_sm * c->sm_count));
-  cf.launch(c->T, P, grid, threads, smem, (cudaStream_t)stream);
+  cf.launch(c->Tu, P, grid, threads, smem, (cudaStream_t)stream);
   CK(cudaGetLastError());
   return DDHDG_OK;
 }
@@ -1857,7 +1865,7 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
 
   // the status word must start at zero (a singular local system sets it)
   CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), (cudaStream_t)stream));
-  cf.launch(c->T, P, grid, threads, smem, (cudaStream_t)stream);
+  cf.launch(c->Tu, P, grid, threads, smem, (cudaStream_t)stream);
   CK(cudaGetLastError());
   return DDHDG_OK;
 }
@@ -2146,6 +2154,504 @@ ddhdg_reconstruct_plain(ddhdg_ctx *c, const double *cell_state, const double *tr
   A.update_trace = update_trace;
   A.update_cell  = update_cell;
   return plain_run(c, thermo, P, A, c->ncells, (cudaStream_t)stream);
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched condensation / reconstruction over many contexts (devices of
+// different mesh sizes and degrees, one dimension): one persistent launch
+// each, consuming a work list of tiles; tile shapes from an autotuner.
+
+struct ddhdg_batch
+{
+  int                      dim = 0, n = 0, thermo = 0;
+  std::vector<ddhdg_ctx *> ctx;
+  std::vector<BatchJob>    jobs;
+  std::vector<int64_t>     ncells, ycache_off;
+  std::vector<double>      cost_per_cell; // per job, for the heaviest-first order
+  DevBuf<unsigned char>    d_jobs, d_tiles_c, d_tiles_r;
+  DevBuf<double>           ycache, rscratch;
+  DevBuf<int>              counter; // [0]: condense, [1]: reconstruct
+  bool                     degrees[4]        = {false, false, false, false};
+  int                      cells_per_tile[4] = {0, 32, 32, 4};
+  int                      ctas_per_sm       = 2;
+  int                      rcells_per_tile   = 256;
+  int                      ntiles_c = 0, ntiles_r = 0, grid_c = 0, grid_r = 0;
+  size_t                   smem_c = 0, smem_r = 0;
+  bool                     any_r_global         = false;
+  int                      max_rscratch_per_cta = 0;
+  int                      sm_count             = 148;
+  cudaStream_t             cap                  = nullptr;
+  cudaGraphExec_t          g_c = nullptr, g_r = nullptr;
+  ~ddhdg_batch()
+  {
+    if (g_c)
+      cudaGraphExecDestroy(g_c);
+    if (g_r)
+      cudaGraphExecDestroy(g_r);
+    if (cap)
+      cudaStreamDestroy(cap);
+  }
+};
+
+namespace
+{
+  const void *
+  batch_condense_fn(int dim)
+  {
+    switch (dim)
+      {
+        case 1: return reinterpret_cast<const void *>(batch_condense_kernel<1>);
+        case 2: return reinterpret_cast<const void *>(batch_condense_kernel<2>);
+        default: return reinterpret_cast<const void *>(batch_condense_kernel<3>);
+      }
+  }
+  const void *
+  batch_reconstruct_fn(int dim)
+  {
+    switch (dim)
+      {
+        case 1: return reinterpret_cast<const void *>(batch_reconstruct_kernel<1>);
+        case 2: return reinterpret_cast<const void *>(batch_reconstruct_kernel<2>);
+        default: return reinterpret_cast<const void *>(batch_reconstruct_kernel<3>);
+      }
+  }
+
+  // the unit-cell constant tables of every warp-per-cell degree of DIM
+  template <int D>
+  void
+  fill_batch_tabs(BatchTabs<D> &C)
+  {
+    const double unit[3] = {1., 1., 1.};
+    if constexpr (batch_warp<D, 1>)
+      fill_ctab(build_tables(D, 1, unit), C.t1);
+    if constexpr (batch_warp<D, 2>)
+      fill_ctab(build_tables(D, 2, unit), C.t2);
+    if constexpr (batch_warp<D, 3>)
+      fill_ctab(build_tables(D, 3, unit), C.t3);
+  }
+
+  // work lists and launch shapes for the current tile sizes
+  int
+  batch_plan(ddhdg_batch *b)
+  {
+    if (b->g_c)
+      {
+        cudaGraphExecDestroy(b->g_c);
+        b->g_c = nullptr;
+      }
+    if (b->g_r)
+      {
+        cudaGraphExecDestroy(b->g_r);
+        b->g_r = nullptr;
+      }
+    std::vector<BatchTile> tc, tr;
+    for (int j = 0; j < b->n; ++j)
+      {
+        const int     k  = b->jobs[j].k;
+        const int64_t nc = b->ncells[j];
+        const int64_t T  = std::max(1, b->cells_per_tile[k]);
+        for (int64_t c0 = 0; c0 < nc; c0 += T)
+          tc.push_back(BatchTile{j, 0, c0, std::min(nc, c0 + T)});
+        for (int64_t c0 = 0; c0 < nc; c0 += b->rcells_per_tile)
+          tr.push_back(BatchTile{j, 0, c0, std::min<int64_t>(nc, c0 + b->rcells_per_tile)});
+      }
+    // heaviest tiles first, so that the last tiles handed out are short
+    auto cost = [b](const BatchTile &t) { return (double)(t.end - t.begin) * b->cost_per_cell[t.job]; };
+    std::stable_sort(tc.begin(), tc.end(),
+                     [&](const BatchTile &x, const BatchTile &y) { return cost(x) > cost(y); });
+    int r;
+    if ((r = b->d_tiles_c.upload(reinterpret_cast<const unsigned char *>(tc.data()), tc.size() * sizeof(BatchTile))))
+      return r;
+    if ((r = b->d_tiles_r.upload(reinterpret_cast<const unsigned char *>(tr.data()), tr.size() * sizeof(BatchTile))))
+      return r;
+    b->ntiles_c     = (int)tc.size();
+    b->ntiles_r     = (int)tr.size();
+    const void *fc = batch_condense_fn(b->dim), *fr = batch_reconstruct_fn(b->dim);
+    CK(allow_full_dynamic_smem(fc));
+    CK(allow_full_dynamic_smem(fr));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fc, BatchTPB, b->smem_c));
+    if (per_sm < 1)
+      return fail(DDHDG_BAD_ARG, "batched condense kernel does not fit on an SM");
+    b->grid_c = std::max(1, std::min(b->ntiles_c, std::min(per_sm, b->ctas_per_sm) * b->sm_count));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fr, BatchRTPB, b->smem_r));
+    if (per_sm < 1)
+      return fail(DDHDG_BAD_ARG, "batched reconstruction kernel does not fit on an SM");
+    b->grid_r = std::max(1, std::min(b->ntiles_r, per_sm * b->sm_count));
+    // R blocks outside shared memory (3D degree 2): one slice per CTA
+    if (b->any_r_global)
+      {
+        if ((r = b->rscratch.alloc((size_t)b->grid_c * b->max_rscratch_per_cta)))
+          return r;
+        for (auto &J : b->jobs)
+          if (J.P.rscratch)
+            J.P.rscratch = b->rscratch.p;
+        if ((r = b->d_jobs.upload(reinterpret_cast<const unsigned char *>(b->jobs.data()),
+                                  b->jobs.size() * sizeof(BatchJob))))
+          return r;
+      }
+    return DDHDG_OK;
+  }
+
+  int
+  batch_launch_condense(ddhdg_batch *b, cudaStream_t s)
+  {
+    CK(cudaMemsetAsync(b->counter.p, 0, sizeof(int), s));
+    const BatchJob  *jobs  = reinterpret_cast<const BatchJob *>(b->d_jobs.p);
+    const BatchTile *tiles = reinterpret_cast<const BatchTile *>(b->d_tiles_c.p);
+    switch (b->dim)
+      {
+        case 1:
+          {
+            static BatchTabs<1> C; // filled once; the tables do not depend on the device
+            static std::once_flag once;
+            std::call_once(once, [] { fill_batch_tabs<1>(C); });
+            batch_condense_kernel<1><<<b->grid_c, BatchTPB, b->smem_c, s>>>(jobs, tiles, b->ntiles_c, b->counter.p, C);
+          }
+          break;
+        case 2:
+          {
+            static BatchTabs<2> C;
+            static std::once_flag once;
+            std::call_once(once, [] { fill_batch_tabs<2>(C); });
+            batch_condense_kernel<2><<<b->grid_c, BatchTPB, b->smem_c, s>>>(jobs, tiles, b->ntiles_c, b->counter.p, C);
+          }
+          break;
+        default:
+          {
+            static BatchTabs<3> C;
+            static std::once_flag once;
+            std::call_once(once, [] { fill_batch_tabs<3>(C); });
+            batch_condense_kernel<3><<<b->grid_c, BatchTPB, b->smem_c, s>>>(jobs, tiles, b->ntiles_c, b->counter.p, C);
+          }
+          break;
+      }
+    CK(cudaGetLastError());
+    return DDHDG_OK;
+  }
+
+  int
+  batch_launch_reconstruct(ddhdg_batch *b, cudaStream_t s)
+  {
+    CK(cudaMemsetAsync(b->counter.p + 1, 0, sizeof(int), s));
+    const BatchJob  *jobs  = reinterpret_cast<const BatchJob *>(b->d_jobs.p);
+    const BatchTile *tiles = reinterpret_cast<const BatchTile *>(b->d_tiles_r.p);
+    int             *cnt   = b->counter.p + 1;
+    switch (b->dim)
+      {
+        case 1:
+          batch_reconstruct_kernel<1><<<b->grid_r, BatchRTPB, b->smem_r, s>>>(jobs, tiles, b->ntiles_r, cnt);
+          break;
+        case 2:
+          batch_reconstruct_kernel<2><<<b->grid_r, BatchRTPB, b->smem_r, s>>>(jobs, tiles, b->ntiles_r, cnt);
+          break;
+        default:
+          batch_reconstruct_kernel<3><<<b->grid_r, BatchRTPB, b->smem_r, s>>>(jobs, tiles, b->ntiles_r, cnt);
+          break;
+      }
+    CK(cudaGetLastError());
+    return DDHDG_OK;
+  }
+
+  // replay of the launch from a CUDA graph captured on the first call (on
+  // an internal stream, thread-local capture); eager launch if capture fails
+  int
+  batch_run(ddhdg_batch *b, cudaStream_t s, bool recon)
+  {
+    cudaGraphExec_t &ge = recon ? b->g_r : b->g_c;
+    if (!ge)
+      {
+        if (!b->cap)
+          CK(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess)
+          {
+            const int         rr = recon ? batch_launch_reconstruct(b, b->cap) : batch_launch_condense(b, b->cap);
+            const cudaError_t e  = cudaStreamEndCapture(b->cap, &g);
+            if (rr == DDHDG_OK && e == cudaSuccess && g)
+              {
+                if (cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+                  ge = nullptr;
+              }
+            if (g)
+              cudaGraphDestroy(g);
+          }
+        cudaGetLastError();
+      }
+    if (ge)
+      {
+        CK(cudaGraphLaunch(ge, s));
+        return DDHDG_OK;
+      }
+    return recon ? batch_launch_reconstruct(b, s) : batch_launch_condense(b, s);
+  }
+
+  // best of `reps` eager launches of the batched condensation (after one
+  // warm-up launch), by CUDA events on s
+  int
+  batch_time(ddhdg_batch *b, cudaStream_t s, int reps, float &ms)
+  {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int   r    = batch_launch_condense(b, s);
+    float best = 1e30f;
+    for (int i = 0; i < reps && r == DDHDG_OK; ++i)
+      {
+        cudaEventRecord(e0, s);
+        r = batch_launch_condense(b, s);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess)
+          r = fail(DDHDG_CUDA_ERROR, "batched condense launch failed");
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        best = std::min(best, t);
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ms = best;
+    return r;
+  }
+} // namespace
+
+extern "C" {
+
+int
+ddhdg_batch_create(const ddhdg_batch_item *items, int n, int thermo, ddhdg_batch **out)
+{
+  if (!items || n < 1 || !out)
+    return fail(DDHDG_BAD_ARG, "null argument or empty batch");
+  thermo = thermo ? 1 : 0;
+  std::unique_ptr<ddhdg_batch> b(new ddhdg_batch);
+  b->n      = n;
+  b->thermo = thermo;
+  b->dim    = items[0].ctx ? items[0].ctx->dim : 0;
+  int64_t                    ytotal = 0;
+  int                        r;
+  for (int j = 0; j < n; ++j)
+    {
+      const ddhdg_batch_item &it = items[j];
+      ddhdg_ctx              *c  = it.ctx;
+      if (!c || !it.cell_state || !it.trace_state || !it.tt || !it.rhs || !it.dflag || !it.dval)
+        return fail(DDHDG_BAD_ARG, "batch item " + std::to_string(j) + ": null argument");
+      if (c->dim != b->dim)
+        return fail(DDHDG_BAD_ARG, "batch items must share one dimension");
+      if (c->desc.precision != 0)
+        return fail(DDHDG_BAD_ARG, "the batched launch is FP64 (item " + std::to_string(j) +
+                                     " has a mixed-precision context)");
+      Mode &m = c->mode[thermo];
+      if (!m.built)
+        set_mode_comps(c, thermo); // host bookkeeping only
+      b->ctx.push_back(c);
+      b->ncells.push_back(c->ncells);
+      b->sm_count = c->sm_count;
+      BatchJob J{};
+      J.P             = make_params(c, thermo);
+      J.P.cell0       = 0;
+      J.P.ncells      = c->ncells;
+      J.P.cell_state  = it.cell_state;
+      J.P.trace_state = it.trace_state;
+      J.P.tt          = it.tt;
+      J.P.rhs         = it.rhs;
+      J.P.dflag       = it.dflag;
+      J.P.dval        = it.dval;
+      J.dtrace        = it.update_trace;
+      J.dcell         = it.update_cell;
+      J.k             = c->k;
+      const int Ns    = m.ncomp * c->nb;
+      b->ycache_off.push_back(ytotal);
+      ytotal += ((c->ncells * Ns * m.ycols) + 31) & ~(int64_t)31;
+      b->degrees[c->k] = true;
+      // Ns^3 (inverse) + Ns^2 (1 + Nt) (Y) + Nt^2 Ns (tt): heaviest-first order
+      b->cost_per_cell.push_back((double)Ns * Ns * Ns + (double)Ns * Ns * (1 + m.Nt) +
+                                 (double)m.Nt * m.Nt * Ns);
+      if (3 * c->nb <= 32)
+        {
+          const Ws3Off w = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, 8);
+          b->smem_c      = std::max(b->smem_c, (size_t)BatchWarp * w.total * sizeof(double));
+          J.P.wpb        = 1;
+          J.P.stage      = 0;
+        }
+      else
+        {
+          // the tables are read through L1 (not staged) and the chunk of
+          // trace columns is the largest that keeps two CTAs on an SM; R
+          // moves to global memory only when nothing else fits (neither
+          // choice changes the arithmetic)
+          int    chunk = 0;
+          bool   r_global = false;
+          size_t smem     = 0;
+          for (size_t limit : {(size_t)110 * 1024, (size_t)220 * 1024})
+            {
+              for (int rg = 0; rg < 2 && !chunk; ++rg)
+                for (int ch = 16; ch >= 1 && !chunk; ch /= 2)
+                  {
+                    const Ws2Off w = ws2_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, ch, rg != 0);
+                    if ((size_t)w.total * sizeof(double) <= limit)
+                      {
+                        chunk    = ch;
+                        r_global = rg != 0;
+                        smem     = (size_t)w.total * sizeof(double);
+                      }
+                  }
+              if (chunk)
+                break;
+            }
+          if (!chunk)
+            return fail(DDHDG_BAD_ARG, "the per-cell workspace does not fit in shared memory");
+          J.P.wpb   = 1;
+          J.P.chunk = chunk;
+          J.P.stage = 0;
+          b->smem_c = std::max(b->smem_c, smem);
+          if (r_global)
+            {
+              b->any_r_global         = true;
+              b->max_rscratch_per_cta = std::max(b->max_rscratch_per_cta, Ns * m.ncol);
+              J.P.rscratch            = reinterpret_cast<double *>(1); // set by batch_plan
+            }
+        }
+      // reconstruction workspace (reconstruct_cells with BatchRTPB / 32 warps)
+      const size_t nPQ = (size_t)(c->to.minv - c->to.P);
+      const int    wsz = (Ns + 2 * c->F * 3 * c->nf + c->nb + m.Nt + 1) & ~1;
+      b->smem_r = std::max(b->smem_r,
+                           (((nPQ + 1) & ~(size_t)1) + (size_t)(BatchRTPB / 32) * wsz) * sizeof(double));
+      b->jobs.push_back(J);
+    }
+  if ((r = b->ycache.alloc((size_t)ytotal)))
+    return r;
+  for (int j = 0; j < n; ++j)
+    b->jobs[j].P.ycache = b->ycache.p + b->ycache_off[j];
+  if ((r = b->counter.alloc(2)))
+    return r;
+  if ((r = b->d_jobs.upload(reinterpret_cast<const unsigned char *>(b->jobs.data()),
+                            b->jobs.size() * sizeof(BatchJob))))
+    return r;
+  if ((r = batch_plan(b.get())))
+    return r;
+  *out = b.release();
+  return DDHDG_OK;
+}
+
+int
+ddhdg_batch_destroy(ddhdg_batch *b)
+{
+  delete b;
+  return DDHDG_OK;
+}
+
+int
+ddhdg_batch_condense(ddhdg_batch *b, ddhdg_stream_t stream)
+{
+  if (!b)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  return batch_run(b, (cudaStream_t)stream, false);
+}
+
+int
+ddhdg_batch_reconstruct(ddhdg_batch *b, ddhdg_stream_t stream)
+{
+  if (!b)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  for (const auto &J : b->jobs)
+    if (!J.dtrace || !J.dcell)
+      return fail(DDHDG_BAD_ARG, "a batch item has no update_trace / update_cell");
+  return batch_run(b, (cudaStream_t)stream, true);
+}
+
+int
+ddhdg_batch_set_shape(ddhdg_batch *b, const int *cells_per_tile, int ctas_per_sm)
+{
+  if (!b || !cells_per_tile || ctas_per_sm < 1)
+    return fail(DDHDG_BAD_ARG, "null argument or no CTA per SM");
+  for (int k = 1; k <= 3; ++k)
+    if (cells_per_tile[k - 1] < 1)
+      return fail(DDHDG_BAD_ARG, "cells per tile must be positive");
+  for (int k = 1; k <= 3; ++k)
+    b->cells_per_tile[k] = cells_per_tile[k - 1];
+  b->ctas_per_sm = ctas_per_sm;
+  return batch_plan(b);
+}
+
+int
+ddhdg_batch_get_shape(const ddhdg_batch *b, int *cells_per_tile, int *ctas_per_sm, int *grid,
+                      int *ntiles)
+{
+  if (!b)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  for (int k = 1; k <= 3 && cells_per_tile; ++k)
+    cells_per_tile[k - 1] = b->cells_per_tile[k];
+  if (ctas_per_sm)
+    *ctas_per_sm = b->ctas_per_sm;
+  if (grid)
+    *grid = b->grid_c;
+  if (ntiles)
+    *ntiles = b->ntiles_c;
+  return DDHDG_OK;
+}
+
+int
+ddhdg_batch_autotune(ddhdg_batch *b, int reps, float *best_ms, ddhdg_stream_t stream)
+{
+  if (!b)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  reps           = std::max(1, reps);
+  cudaStream_t s = (cudaStream_t)stream;
+  int          r;
+  float        best = 0.f;
+  if ((r = batch_time(b, s, reps, best)))
+    return r;
+  // coordinate search: the tile size of each degree present (heaviest
+  // degree first), then the CTAs per SM
+  const int warp_cand[] = {4, 8, 16, 32, 64, 128, 256};
+  const int cta_cand[]  = {1, 2, 4, 8, 16, 32};
+  for (int k = 3; k >= 1; --k)
+    {
+      if (!b->degrees[k])
+        continue;
+      int nbk = 1;
+      for (int a = 0; a < b->dim; ++a)
+        nbk *= k + 1;
+      const bool cta  = 3 * nbk > 32;
+      const int *cand = cta ? cta_cand : warp_cand;
+      const int  nc   = cta ? 6 : 7;
+      int        keep = b->cells_per_tile[k];
+      for (int i = 0; i < nc; ++i)
+        {
+          if (cand[i] == keep)
+            continue;
+          b->cells_per_tile[k] = cand[i];
+          float t              = 0.f;
+          if ((r = batch_plan(b)) || (r = batch_time(b, s, reps, t)))
+            return r;
+          if (t < best)
+            {
+              best = t;
+              keep = cand[i];
+            }
+          b->cells_per_tile[k] = keep;
+        }
+    }
+  for (int cps = 1; cps <= 2; ++cps)
+    {
+      if (cps == b->ctas_per_sm)
+        continue;
+      const int prev = b->ctas_per_sm;
+      b->ctas_per_sm = cps;
+      float t        = 0.f;
+      if ((r = batch_plan(b)) || (r = batch_time(b, s, reps, t)))
+        return r;
+      if (t < best)
+        best = t;
+      else
+        b->ctas_per_sm = prev;
+    }
+  if ((r = batch_plan(b)))
+    return r;
+  if (best_ms)
+    *best_ms = best;
+  return DDHDG_OK;
 }
 
 } // extern "C"

@@ -90,9 +90,14 @@ namespace ddhdg
     return o;
   }
 
+  // The body of the CTA-per-cell condensation: the CTA (CondenseTPB threads)
+  // works through the cells cell_begin, cell_begin + cell_step, ... <
+  // cell_end with the workspace at smem (tables first when P.stage) and, for
+  // R outside shared memory, the R slice `slot` of P.rscratch.
   template <int DIM, int K>
-  __global__ void __launch_bounds__(CondenseTPB)
-  condense2_kernel(const KParams P)
+  __device__ __forceinline__ void
+  condense2_cells(const KParams &P, double *smem, int64_t slot, int64_t cell_begin,
+                  int64_t cell_end, int64_t cell_step)
   {
     using Dm          = Dims<DIM, K>;
     constexpr int nb  = Dm::nb;
@@ -105,7 +110,6 @@ namespace ddhdg
     constexpr int NCA = Dm::Nc_all;
     constexpr int T   = CondenseTPB;
     constexpr int NW  = T / 32;
-    extern __shared__ double smem[];
     __shared__ int sh_piv;
     __shared__ int sh_sing;
 
@@ -160,7 +164,7 @@ namespace ddhdg
     // R of the largest systems (3D k = 2 with drift columns: 210 KB) lives
     // in this CTA's slice of a global buffer, which stays in L2
     if (P.rscratch)
-      R = P.rscratch + (int64_t)blockIdx.x * Ns * ncol;
+      R = P.rscratch + slot * Ns * ncol;
 
     const double eps = P.eps, mun = P.mun, mup = P.mup, U_T = P.U_T;
     const bool   thermo   = P.thermo != 0;
@@ -172,7 +176,7 @@ namespace ddhdg
       ce_of[P.comps[c]] = c;
     const bool nen = ce_of[1] >= 0, pen = ce_of[2] >= 0;
 
-    for (int64_t cell = P.cell0 + blockIdx.x; cell < P.ncells; cell += gridDim.x)
+    for (int64_t cell = cell_begin; cell < cell_end; cell += cell_step)
       {
         // ------------------------------------------------------ state
         const double *cs = P.cell_state + cell * NCA;
@@ -857,5 +861,13 @@ namespace ddhdg
           }
         __syncthreads();
       }
+  }
+
+  template <int DIM, int K>
+  __global__ void __launch_bounds__(CondenseTPB)
+  condense2_kernel(const KParams P)
+  {
+    extern __shared__ double smem[];
+    condense2_cells<DIM, K>(P, smem, blockIdx.x, P.cell0 + blockIdx.x, P.ncells, gridDim.x);
   }
 } // namespace ddhdg

@@ -49,7 +49,11 @@ namespace ddhdg
 
   // Constant tables read at lane-uniform addresses in fully unrolled loops.
   // They travel as a kernel parameter (constant bank), so that the FMAs take
-  // them as constant operands; at most 14.4 KB (3D, degree 1).
+  // them as constant operands; at most 14.4 KB (3D, degree 1).  They are the
+  // tables of the unit cell: the elimination operators P = M^-1 G and
+  // Q = M^-1 C_W of axis s scale exactly as 1 / h_s, and that factor
+  // (KParams::ih) goes into the per-cell coefficient that multiplies them, so
+  // that devices of every mesh size share one copy.
   template <int DIM, int K>
   struct CTab
   {
@@ -194,9 +198,17 @@ namespace ddhdg
   // the trace-row weights are FP32 and the products accumulate in FP64 on the
   // tensor path, while the state, every residual and the outputs stay FP64
   // (a Newton loop on these blocks converges to the FP64 solution).
-  template <int DIM, int K, typename JT = double>
-  __global__ void __launch_bounds__(Condense3MaxWPB * 32, sizeof(JT) == 8 ? 1 : 2)
-  condense3_kernel(const KParams P, const __grid_constant__ CTab<DIM, K> C)
+  //
+  // The body of the warp-per-cell condensation: one warp works through the
+  // cells cell_begin, cell_begin + cell_step, ... < cell_end with its own
+  // workspace ws (ws3_layout doubles) and pivot list piv [3 (k+1)^d].  The
+  // tables C are the kernel's constant-bank parameter in condense3_kernel
+  // and a per-device copy in global memory in the batched launch; the
+  // arithmetic is the same, so the results are bitwise the same.
+  template <int DIM, int K, typename JT>
+  __device__ __forceinline__ void
+  condense3_cells(const KParams &P, const CTab<DIM, K> &C, double *ws, int *piv,
+                  int64_t cell_begin, int64_t cell_end, int64_t cell_step)
   {
     using Dm            = Dims<DIM, K>;
     constexpr int nb    = Dm::nb;
@@ -210,11 +222,8 @@ namespace ddhdg
     constexpr int NSMAX = 3 * nb;
     constexpr bool RW   = DIM == 3 && sizeof(JT) == 8; // recompute rA / rS / rD (see ws3_layout)
     static_assert(NSMAX <= 32, "one lane per row of the scalar system");
-    extern __shared__ __align__(16) double smem[];
-    __shared__ int piv3[Condense3MaxWPB][NSMAX];
 
     const int  lane  = threadIdx.x & 31;
-    const int  warp  = threadIdx.x >> 5;
     const int  ncomp = P.ncomp;
     const int  Ns    = ncomp * nb;
     const int  Nt    = F * ncomp * nf;
@@ -240,7 +249,6 @@ namespace ddhdg
     const double *QW_f   = tb + P.to.QW_f;
 
     const Ws3Off wo = ws3_layout(DIM, nb, nf, ncomp, ncol, (int)sizeof(JT));
-    double      *ws = smem + warp * wo.total;
     const auto   jp = [ws](int off) { return reinterpret_cast<JT *>(ws + off); };
     double *coef = ws + wo.coef, *lam = ws + wo.lam, *c0 = ws + wo.c0, *W0 = ws + wo.W0,
            *qc = ws + wo.qc, *c0f = ws + wo.c0f, *W0n = ws + wo.W0n, *tr0 = ws + wo.tr0,
@@ -269,10 +277,7 @@ namespace ddhdg
         nen |= cmp_of(c) == 1;
         pen |= cmp_of(c) == 2;
       }
-    const int wpb = blockDim.x >> 5;
-
-    for (int64_t cell = P.cell0 + (int64_t)blockIdx.x * wpb + warp; cell < P.ncells;
-         cell += (int64_t)gridDim.x * wpb)
+    for (int64_t cell = cell_begin; cell < cell_end; cell += cell_step)
       {
         // keeps the table loads inside the cell loop (no hoisting of
         // thousands of loop-invariant values into registers)
@@ -695,7 +700,7 @@ namespace ddhdg
 #pragma unroll
                     for (int s = 0; s < DIM; ++s)
                       {
-                        const double w = kq * TLg[(q * DIM + s) * nb + a];
+                        const double w = kq * TLg[(q * DIM + s) * nb + a] * P.ih[s];
 #pragma unroll
                         for (int t = 0; t < Ft; ++t)
                           acc[t] -= w * C.RQk[(q * DIM + s) * Ft + t];
@@ -704,7 +709,7 @@ namespace ddhdg
 #pragma unroll
                 for (int fq = 0; fq < Fq; ++fq)
                   {
-                    const double w = (double)rhp[fq] * TLf[fq * nb + a];
+                    const double w = (double)rhp[fq] * TLf[fq * nb + a] * P.ih[fq / (nqf * 2)];
 #pragma unroll
                     for (int t = 0; t < Ft; ++t)
                       acc[t] -= w * C.RQr[fq * Ft + t];
@@ -783,7 +788,7 @@ namespace ddhdg
                       {
                         const double tg = TLg[(q * DIM + s) * nb + a];
                         lt += (double)bep[q * DIM + s] * tg;
-                        kt[s] = (double)kap[q] * tg;
+                        kt[s] = (double)kap[q] * tg * P.ih[s];
                       }
 #pragma unroll
                     for (int e = 0; e < nb; ++e)
@@ -798,7 +803,7 @@ namespace ddhdg
                 for (int fq = 0; fq < Fq; ++fq)
                   {
                     const double tf = TLf[fq * nb + a];
-                    const double g_ = (double)gap[fq] * tf, r_ = (double)rhp[fq] * tf;
+                    const double g_ = (double)gap[fq] * tf, r_ = (double)rhp[fq] * tf * P.ih[fq / (nqf * 2)];
 #pragma unroll
                     for (int e = 0; e < nb; ++e)
                       acc[e] += g_ * C.phi_f[fq * nb + e] + r_ * C.RTr[fq * nb + e];
@@ -877,7 +882,7 @@ namespace ddhdg
                 mypos = j;
               }
             if (lane == 0)
-              piv3[warp][j] = bl;
+              piv[j] = bl;
             __syncwarp();
           }
         if (sing && lane == 0)
@@ -888,7 +893,7 @@ namespace ddhdg
           JT dsc[NSMAX];
 #pragma unroll
           for (int k = 0; k < NSMAX; ++k)
-            dsc[k] = __shfl_sync(0xffffffffu, rscale, piv3[warp][k]);
+            dsc[k] = __shfl_sync(0xffffffffu, rscale, piv[k]);
 #pragma unroll
           for (int k = 0; k < NSMAX; ++k)
             srow[k] *= dsc[k];
@@ -919,7 +924,7 @@ namespace ddhdg
               for (int ks = 0; ks < KP / 4; ++ks)
                 {
                   const int kk = ks * 4 + tq;
-                  bf[ks] = (kk < Ns && col < ncol) ? (double)R[piv3[warp][kk] * ldr + col] : 0.;
+                  bf[ks] = (kk < Ns && col < ncol) ? (double)R[piv[kk] * ldr + col] : 0.;
                 }
               double acc[MP / 8][2];
 #pragma unroll
@@ -1168,5 +1173,19 @@ namespace ddhdg
         }
         __syncwarp();
       }
+  }
+
+  template <int DIM, int K, typename JT = double>
+  __global__ void __launch_bounds__(Condense3MaxWPB * 32, sizeof(JT) == 8 ? 1 : 2)
+  condense3_kernel(const KParams P, const __grid_constant__ CTab<DIM, K> C)
+  {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int piv3[Condense3MaxWPB][3 * Dims<DIM, K>::nb];
+    const int      warp = threadIdx.x >> 5;
+    const int      wpb  = blockDim.x >> 5;
+    const Ws3Off   wo   = ws3_layout(DIM, Dims<DIM, K>::nb, Dims<DIM, K>::nf, P.ncomp, P.ncol, (int)sizeof(JT));
+    condense3_cells<DIM, K, JT>(P, C, smem + warp * wo.total, piv3[warp],
+                                P.cell0 + (int64_t)blockIdx.x * wpb + warp, P.ncells,
+                                (int64_t)gridDim.x * wpb);
   }
 } // namespace ddhdg

@@ -27,6 +27,7 @@ namespace ddhdg
     int64_t cell0;
     int64_t face_off[3];
     int     face_ext[3][3];
+    double  ih[3]; // 1 / cell size per axis (scales the unit-cell CTab operators)
     // tables (device, global) and their layout
     const double *tables;
     TabOff        to;
@@ -93,17 +94,20 @@ namespace ddhdg
   // Cell update from the trace update: du = Y0 - Y_t dlam for the scalar
   // unknowns, and the flux unknowns from the (linear) flux rows,
   // W_new = P u_new - Q lam_new, i.e. dW = P(u0+du) - W0 - Q(lam0+dlam).
+  //
+  // The body: the whole CTA stages P and Q, then every warp works through the
+  // cells cell_begin + warp * warp_step, then + cell_step, ... < cell_end.
   template <int DIM, int K>
-  __global__ void __launch_bounds__(256, 8) // 8 CTAs per SM: memory-latency bound
-  reconstruct_kernel(const KParams P, const double *__restrict__ dtrace,
-                     double *__restrict__ dcell)
+  __device__ __forceinline__ void
+  reconstruct_cells(const KParams &P, const double *__restrict__ dtrace,
+                    double *__restrict__ dcell, double *smem, int64_t cell_begin,
+                    int64_t warp_step, int64_t cell_end, int64_t cell_step)
   {
     using Dm          = Dims<DIM, K>;
     constexpr int nb  = Dm::nb;
     constexpr int nf  = Dm::nf;
     constexpr int F   = Dm::F;
     constexpr int NCA = Dm::Nc_all;
-    extern __shared__ double smem[];
     const int lane  = threadIdx.x & 31;
     const int warp  = threadIdx.x >> 5;
     const int ncomp = P.ncomp;
@@ -124,8 +128,7 @@ namespace ddhdg
     double *unew = lnew + F * 3 * nf;
     double *dlr  = unew + nb;        // [Nt] trace update, restricted order
 
-    for (int64_t cell = P.cell0 + (int64_t)blockIdx.x * P.wpb + warp; cell < P.ncells;
-         cell += (int64_t)gridDim.x * P.wpb)
+    for (int64_t cell = cell_begin + warp * warp_step; cell < cell_end; cell += cell_step)
       {
         // the cell's face ids: one lane per face, then shuffled (the loop
         // runs the same number of times on every lane)
@@ -202,5 +205,15 @@ namespace ddhdg
             __syncwarp();
           }
       }
+  }
+
+  template <int DIM, int K>
+  __global__ void __launch_bounds__(256, 8) // 8 CTAs per SM: memory-latency bound
+  reconstruct_kernel(const KParams P, const double *__restrict__ dtrace,
+                     double *__restrict__ dcell)
+  {
+    extern __shared__ double smem[];
+    reconstruct_cells<DIM, K>(P, dtrace, dcell, smem, P.cell0 + (int64_t)blockIdx.x * P.wpb, 1,
+                              P.ncells, (int64_t)gridDim.x * P.wpb);
   }
 } // namespace ddhdg

@@ -98,3 +98,24 @@ def bias_sweep(solver, problem, biases, absolute_tol=None, relative_tol=None,
         if callback is not None:
             callback(float(v), solver, res)
     return out
+
+
+def batch_diodes(n, seed=3, sizes=(16, 128), degrees=(1, 2, 3), doping=(1e21, 1e24), junction=(0.3, 0.7),
+                 dim=2):
+    """Seeded heterogeneous batch of diodes shaped like the batched benchmark
+    configuration: mesh cells per side uniform in `sizes`, degree uniform in
+    `degrees`, doping (N_D = N_A) log-uniform in `doping`, junction position
+    uniform in `junction` (fraction of the length).  Returns a list of
+    (problem, parameters, adimensionalizer, spec dict)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        m = int(rng.integers(sizes[0], sizes[1] + 1))
+        k = int(rng.choice(degrees))
+        N = float(10 ** rng.uniform(math.log10(doping[0]), math.log10(doping[1])))
+        xj = float(rng.uniform(*junction))
+        pb, prm, adim = diode(dim=dim, m=m, k=k, N_D=N, N_A=N, x_j=xj)
+        out.append((pb, prm, adim, dict(m=m, k=k, doping=N, x_j=xj)))
+    return out

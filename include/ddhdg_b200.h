@@ -334,6 +334,45 @@ int ddhdg_sample_points(ddhdg_ctx *ctx, const double *cell_state,
 int ddhdg_reference_points(int dim, int degree, double *qref_c, double *qref_f,
                            double *support);
 
+/* ---------------------------------------------------------------------
+ * Batched launches over many contexts: devices (diodes) of different mesh
+ * sizes and degrees, of one dimension, condensed in ONE persistent launch
+ * per Newton step, and reconstructed in one more.  The reference runs its
+ * per-cell worker over one device's cells at a time (WorkStream,
+ * include/assembling_methods.template.h:67-88); a batch hands out tiles
+ * (device, range of its cells) from a work list to the CTAs of one grid.
+ * Every device's outputs are bitwise those of its own
+ * ddhdg_assemble_condense / ddhdg_reconstruct.  FP64 contexts only.  The
+ * pointers of an item are fixed for the life of the batch (the launches
+ * are replayed from CUDA graphs); the batch keeps its own reconstruction
+ * data, so ddhdg_batch_reconstruct follows ddhdg_batch_condense. */
+typedef struct ddhdg_batch ddhdg_batch;
+typedef struct ddhdg_batch_item
+{
+  ddhdg_ctx    *ctx;
+  const double *cell_state, *trace_state; /* device state of this context */
+  double       *tt, *rhs;                 /* condensation outputs, as in  */
+  int32_t      *dflag;                    /* ddhdg_assemble_condense      */
+  double       *dval;
+  const double *update_trace; /* reconstruction input (or NULL)  */
+  double       *update_cell;  /* reconstruction output (or NULL) */
+} ddhdg_batch_item;
+
+int ddhdg_batch_create(const ddhdg_batch_item *items, int nitems, int thermo_eq,
+                       ddhdg_batch **batch);
+int ddhdg_batch_destroy(ddhdg_batch *batch);
+int ddhdg_batch_condense(ddhdg_batch *batch, ddhdg_stream_t stream);
+int ddhdg_batch_reconstruct(ddhdg_batch *batch, ddhdg_stream_t stream);
+/* Tile shape: cells per tile for degrees 1, 2, 3 (cells_per_tile[3]) and
+ * CTAs per SM.  ddhdg_batch_autotune picks them by timing the batch's own
+ * condensation launch (coordinate search, best of `reps` launches per
+ * candidate, on `stream`; the outputs are written by every launch) and
+ * returns the best time in ms. */
+int ddhdg_batch_set_shape(ddhdg_batch *batch, const int *cells_per_tile, int ctas_per_sm);
+int ddhdg_batch_get_shape(const ddhdg_batch *batch, int *cells_per_tile, int *ctas_per_sm,
+                          int *grid, int *ntiles);
+int ddhdg_batch_autotune(ddhdg_batch *batch, int reps, float *best_ms, ddhdg_stream_t stream);
+
 /* Last error message of the calling thread (static storage). */
 const char *ddhdg_last_error(void);
 

@@ -55,11 +55,16 @@ def block_rel_errs(tt, rhs, S, g, o, thermo=False):
     |cc_rhs| (``condense_solve_scale``): in 3D Dirichlet cells cc^-1 cc_rhs
     is itself a cancellation of terms ~4e6 times larger than the V block of
     the result, which no FP64 solve resolves below ~1e-9 of that block.
-    Returns (worst tt ratio, worst rhs ratio, per-block table)."""
+    A block that vanishes in exact arithmetic (V rows against n columns with
+    phi_linearize) holds only round-off of the other blocks: its scale is
+    floored at 1e-8 of the largest block's, so it is checked to 1e-18 of
+    that.  Returns (worst tt ratio, worst rhs ratio, per-block table)."""
     tt = np.asarray(tt).reshape(S.shape)
     rhs = np.asarray(rhs).reshape(g.shape)
     bt, br = o.condense_block_scale
     _, sr = o.condense_solve_scale
+    bt = np.maximum(bt, 1e-8 * bt.max())
+    sr = np.maximum(sr, 1e-8 * sr.max())
     ncomp = bt.shape[0]
     comp = (np.arange(S.shape[1]) // o.nf) % ncomp
     table = {}

@@ -6,9 +6,10 @@
   restatement of the reference's assembly
   (include/assembling_methods.template.h:134-2160, local_condenser.cpp:
   142-160).  Each array is split into blocks by (component, flux or scalar)
-  of its rows and columns, and every block is checked at 1e-12 of its own
+  of its rows and columns, and every block is checked at 1e-10 of its own
   largest magnitude: the assembly sums a handful of quadrature terms, so the
-  differences are FP64 round-off of those terms.
+  differences are FP64 round-off of those terms (up to a few 1e-12 of the
+  block where the terms cancel, e.g. the flux rows of c, V0 div q - E0 . q).
 * ddhdg_assemble_condense_plain / ddhdg_reconstruct_plain (the full local
   system, LU of cc, Schur complement, and the second assembly pass of the
   reconstruction) against the oracle's accurate condensation, per block at
@@ -24,7 +25,7 @@ from tests.gpu_helpers import block_rel_errs, cell_block_rel_err, make_pair
 
 pytestmark = pytest.mark.gpu
 
-TOL_ASSEMBLY = 1e-12
+TOL_ASSEMBLY = 1e-10
 TOL = 1e-10
 
 

@@ -61,6 +61,12 @@ def test_quasi_fermi_potentials_match_oracle():
     V = o.evaluate(0, pts)
     for c, comp in ((1, Component.phi_n), (2, Component.phi_p)):
         dens = o.evaluate(c, pts)
-        ref = _qf(c, V, dens, pb)
+        with np.errstate(invalid="ignore"):
+            ref = _qf(c, V, dens, pb)
         got = g.evaluate(comp, pts)
-        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max() + 1e-12, comp
+        # the perturbed density interpolates below zero at a few points: no
+        # potential there, on either side
+        ok = dens > 0
+        assert ok.sum() > 0.9 * ok.size
+        assert np.array_equal(np.isnan(got), ~ok), comp
+        assert np.abs(got[ok] - ref[ok]).max() <= 1e-12 * np.abs(ref[ok]).max() + 1e-12, comp
