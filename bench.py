@@ -388,6 +388,107 @@ def run_bias_sweep(args):
     print(json.dumps(line))
 
 
+def run_batch(args):
+    """The batched configuration: a seeded batch of 2D diodes (mesh cells per
+    side uniform in 16..128, degree uniform in {1, 2, 3}, doping log-uniform
+    in 1e21..1e24 m^-3, junction uniform in 0.3..0.7), condensed in ONE
+    persistent launch per Newton step and reconstructed in one more
+    (ddhdg_batch_*, tile shapes from the autotuner, replayed from CUDA
+    graphs), FP64.  Timed with CUDA events over `steps` batch steps; next to
+    it the same work as one launch per device (a batch of one per device) on
+    the first `compare` devices, and the batch of those devices alone."""
+    import torch
+
+    from ddhdg_b200 import _lib
+    from ddhdg_b200 import workloads as cases
+    from ddhdg_b200.batch import CondenseBatch
+    from ddhdg_b200.solver import NPSolver
+
+    t0 = time.perf_counter()
+    specs = cases.batch_diodes(args.batch_devices, seed=2025)
+    solvers = []
+    for pb, prm, adim, _ in specs:
+        g = NPSolver(pb, prm, adim)
+        g.compute_local_charge_neutrality()
+        for c in (1, 2):
+            _lib.check(g.L.ddhdg_project_density(g._ctx, c, 0.0, g.cell_state.data_ptr(),
+                                                 g.trace_state.data_ptr(), g._sp()), "project_density")
+        solvers.append(g)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    batch = CondenseBatch(solvers)
+    for i, g in enumerate(solvers):
+        batch.update_trace[i].fill_(1e-6)
+    t0 = time.perf_counter()
+    tuned_ms = batch.autotune(reps=2)
+    t_tune = time.perf_counter() - t0
+    stream = batch.stream
+
+    def timed(fn, steps):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    steps = max(3, min(args.steps, 20))
+    sampler = ClockSampler(0)
+    sampler.start()
+    cond_ms = timed(batch.condense, steps)
+    rec_ms = timed(batch.reconstruct, steps)
+    clocks = sampler.stop()
+    cells = batch.cells
+    # the same devices' work as one launch per device, on a subset
+    nsub = min(args.batch_compare, len(solvers))
+    sub = solvers[:nsub]
+    sub_batch = CondenseBatch(sub)
+    sub_batch.autotune(reps=2)
+    singles = [CondenseBatch([g]) for g in sub]
+    for b in singles:
+        b.autotune(reps=1)
+    sub_ms = timed(sub_batch.condense, steps)
+
+    def each():
+        for b in singles:
+            b.condense()
+
+    each_ms = timed(each, steps)
+    sub_cells = sum(g.ncells for g in sub)
+    # algorithmic FP64 flops of the condensation (LU form on the full cell
+    # system) summed over the devices, against the DGEMM rate of this GPU
+    flops = sum(algorithmic_flops_per_cell(2, s[3]["k"]) * (s[3]["m"] ** 2) for s in specs)
+    peak = fp64_peak_tflops(torch.device("cuda:0"))
+    by_k = {}
+    for s in specs:
+        by_k.setdefault(s[3]["k"], [0, 0])
+        by_k[s[3]["k"]][0] += 1
+        by_k[s[3]["k"]][1] += s[3]["m"] ** 2
+    line = {"metric": "HDG cells condensed/s, batched heterogeneous diodes (one launch per Newton step)",
+            "value": cells / ((cond_ms + rec_ms) * 1e-3), "unit": "cells/s", "higher_is_better": True,
+            "n_gpus": 1, "steps": steps, "warmup": max(args.warmup, 3), "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{len(specs)} 2D p-n diodes, cells per side U[16,128], degree U{{1,2,3}}, "
+                                   "doping log-U[1e21,1e24] m^-3, junction U[0.3,0.7], seed 2025",
+                       "cells": cells, "devices_per_degree": {str(k): v[0] for k, v in sorted(by_k.items())},
+                       "cells_per_degree": {str(k): v[1] for k, v in sorted(by_k.items())}},
+            "ms_per_step": cond_ms + rec_ms,
+            "stages_ms": {"condense": cond_ms, "reconstruct": rec_ms},
+            "launches_per_step": 2,
+            "autotune": dict(batch.shape(), best_ms=tuned_ms, seconds=t_tune),
+            "roofline": {"bound": "fp64", "achieved": flops / (cond_ms * 1e-3) / 1e12, "peak": peak,
+                         "unit": "TFLOP/s", "frac": flops / (cond_ms * 1e-3) / 1e12 / peak,
+                         "peak_source": "cuBLAS DGEMM 8192^3 timed in this run",
+                         "algorithmic_flops": flops},
+            "per_device_launches": {"devices": nsub, "cells": sub_cells, "batched_condense_ms": sub_ms,
+                                    "one_launch_per_device_ms": each_ms, "speedup": each_ms / sub_ms},
+            "setup_s": t_setup, "clocks": clocks}
+    print(json.dumps(line))
+
+
 def run_trace_solve(args):
     """The global FP64 trace solve alone (ddhdg_solve_condensed: nested-
     dissection multifrontal LU on the device) on the condensed system of the
@@ -523,6 +624,11 @@ def main():
                     help="time the global trace solve alone (nested dissection) on the diode's condensed system")
     ap.add_argument("--condense-3d", action="store_true",
                     help="condensation of the 3D 64^3 degree-1 diode at 0.6 V, FP64 and mixed")
+    ap.add_argument("--batch", action="store_true",
+                    help="batched heterogeneous diodes: one persistent condensation launch per Newton step")
+    ap.add_argument("--batch-devices", type=int, default=512)
+    ap.add_argument("--batch-compare", type=int, default=64,
+                    help="devices of the one-launch-per-device comparison")
     ap.add_argument("--cells-per-side", type=int, default=WORKLOAD["m"],
                     help="smaller meshes of the same diode for profiling runs")
     args = ap.parse_args()
@@ -536,6 +642,8 @@ def main():
         return run_trace_solve(args)
     if args.condense_3d:
         return run_condense_3d(args)
+    if args.batch:
+        return run_batch(args)
 
     import torch
     import torch.distributed as dist
