@@ -268,8 +268,9 @@ def run_serve(args):
     torch.cuda.init()
     # warm the library and the kernels once (not part of the stream)
     serving.solve_one(serving.Request(-1, 2, 32, 1, 0.1, 0.0))
-    reqs = serving.poisson_requests(args.serve_requests, args.serve_rate, seed=2024)
-    server = serving.DiodeServer(max_inflight=8)
+    reqs = serving.poisson_requests(args.serve_requests, args.serve_rate, seed=2024,
+                                    sizes_3d=(args.serve_3d_min, args.serve_3d_max))
+    server = serving.DiodeServer(max_inflight=16)
     t0 = time.perf_counter()
     res = server.run(reqs)
     wall = time.perf_counter() - t0
@@ -277,10 +278,13 @@ def run_serve(args):
     line = {"metric": "serve p50/p99 latency (diode solves, continuous batching)",
             "value": st["p99_s"], "unit": "s", "higher_is_better": False, "n_gpus": 1, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "Poisson stream of 2D 32^2..256^2 (k 1-2) and 3D 8^3..16^3 (k 1) diode "
-                                   "solves, bias U[0, 0.8] V, equilibrium + warm-started Newton",
+            "config": {"workload": f"Poisson stream of 2D 32^2..256^2 (k 1-2) and 3D {args.serve_3d_min}^3.."
+                                   f"{args.serve_3d_max}^3 (k 1) diode solves, bias U[0, 0.8] V, equilibrium + "
+                                   "warm-started Newton; kernel-level continuous batching (one condensation "
+                                   "launch per server step over the requests in flight)",
                        "requests": len(reqs), "rate_per_s": args.serve_rate, "seed": 2024,
                        "max_inflight": server.max_inflight},
+            "server_steps": server.steps, "peak_batch": server.peak_batch,
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"],
             "solves_per_s": st["solves_per_s"], "cells_per_s": st["cells_per_s"],
             "converged": st["converged"], "peak_inflight": server.peak_inflight, "wall_s": wall}
@@ -295,14 +299,15 @@ def serve_quick(n=10, rate=4.0, seed=7):
 
     serving.solve_one(serving.Request(-1, 2, 32, 1, 0.1, 0.0))  # warm the kernels
     reqs = serving.poisson_requests(n, rate, seed=seed, sizes_2d=(32, 96), sizes_3d=(8, 12))
-    server = serving.DiodeServer(max_inflight=8)
+    server = serving.DiodeServer(max_inflight=16)
     t0 = time.perf_counter()
     res = server.run(reqs)
     wall = time.perf_counter() - t0
     st = serving.latency_stats(res, wall)
     return {"p50_s": st["p50_s"], "p99_s": st["p99_s"], "solves_per_s": st["solves_per_s"],
             "converged": st["converged"], "requests": n, "rate_per_s": rate, "seed": seed,
-            "peak_inflight": server.peak_inflight, "wall_s": wall,
+            "peak_inflight": server.peak_inflight, "peak_batch": server.peak_batch,
+            "server_steps": server.steps, "wall_s": wall,
             "workload": "Poisson stream of 2D 32^2..96^2 (k 1-2) and 3D 8^3..12^3 (k 1) diode solves, "
                         "bias U[0, 0.8] V (full-size stream: bench.py --serve)"}
 
@@ -616,6 +621,9 @@ def main():
                     help="serve a seeded Poisson stream of diode solves and report p50/p99 latency")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=4.0, help="arrivals per second")
+    ap.add_argument("--serve-3d-min", type=int, default=16)
+    ap.add_argument("--serve-3d-max", type=int, default=24,
+                    help="largest 3D mesh of the stream (the nested-dissection fronts grow as m^5 in 3D)")
     ap.add_argument("--bias-sweep", action="store_true",
                     help="time the warm-started 0..0.8 V sweep (17 points) instead of the step")
     ap.add_argument("--mixed", action="store_true",

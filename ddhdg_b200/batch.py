@@ -27,25 +27,21 @@ class CondenseBatch:
     The solvers' state tensors must stay in place (the launches are replayed
     from CUDA graphs)."""
 
-    def __init__(self, solvers, thermo=False):
-        import torch
-
+    def __init__(self, solvers, thermo=False, buffers=None):
         self.solvers = list(solvers)
         self.thermo = bool(thermo)
         self.L = _lib.load()
-        dev = self.solvers[0].device
-        self.tt, self.rhs, self.dflag, self.dval = [], [], [], []
-        self.update_trace, self.update_cell = [], []
+        if buffers is None:
+            buffers = [self.buffers_for(g, thermo) for g in self.solvers]
+        self.buffers = buffers
+        self.tt = [b["tt"] for b in buffers]
+        self.rhs = [b["rhs"] for b in buffers]
+        self.dflag = [b["dflag"] for b in buffers]
+        self.dval = [b["dval"] for b in buffers]
+        self.update_trace = [b["update_trace"] for b in buffers]
+        self.update_cell = [b["update_cell"] for b in buffers]
         items = (_lib.BatchItem * len(self.solvers))()
         for i, g in enumerate(self.solvers):
-            s = g.sizes(thermo)
-            nc, Nt = g.ncells, s.Nt
-            self.tt.append(torch.empty((nc, Nt, Nt), dtype=torch.float64, device=dev))
-            self.rhs.append(torch.empty((nc, Nt), dtype=torch.float64, device=dev))
-            self.dflag.append(torch.empty((nc, Nt), dtype=torch.int32, device=dev))
-            self.dval.append(torch.empty((nc, Nt), dtype=torch.float64, device=dev))
-            self.update_trace.append(torch.zeros(g.nfaces * 3 * g.nf, dtype=torch.float64, device=dev))
-            self.update_cell.append(torch.empty((nc, g.Nc_all), dtype=torch.float64, device=dev))
             it = items[i]
             it.ctx = g._ctx
             it.cell_state = g.cell_state.data_ptr()
@@ -63,8 +59,43 @@ class CondenseBatch:
         self.stream = self.solvers[0].stream
         self.cells = sum(g.ncells for g in self.solvers)
 
+    @staticmethod
+    def buffers_for(g, thermo=False):
+        """Output and update buffers of one solver in a batch (kept by a
+        caller that rebuilds batches over the same solvers, so that the
+        solvers' trace-solve graphs stay valid)."""
+        import torch
+
+        s = g.sizes(thermo)
+        nc, Nt, dev = g.ncells, s.Nt, g.device
+        return {"tt": torch.empty((nc, Nt, Nt), dtype=torch.float64, device=dev),
+                "rhs": torch.empty((nc, Nt), dtype=torch.float64, device=dev),
+                "dflag": torch.empty((nc, Nt), dtype=torch.int32, device=dev),
+                "dval": torch.empty((nc, Nt), dtype=torch.float64, device=dev),
+                "update_trace": torch.zeros(g.nfaces * 3 * g.nf, dtype=torch.float64, device=dev),
+                "update_cell": torch.empty((nc, g.Nc_all), dtype=torch.float64, device=dev)}
+
     def _sp(self):
         return ctypes.c_void_p(self.stream.cuda_stream)
+
+    def newton_step(self, alphas):
+        """One Newton step of every solver (batched condensation, the trace
+        solves overlapped on side streams, batched reconstruction, damped
+        update in place).  Returns (norms [n][4]: max |update_cell|,
+        max |update_trace|, max |cell_state|, max |trace_state| before the
+        update, statuses [n])."""
+        import numpy as np
+
+        n = len(self.solvers)
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(alphas, dtype=np.float64), (n,)))
+        norms = np.zeros((n, 4))
+        status = (ctypes.c_int * n)()
+        dp = ctypes.POINTER(ctypes.c_double)
+        code = self.L.ddhdg_batch_newton_step(self._b, a.ctypes.data_as(dp), norms.ctypes.data_as(dp), status,
+                                              self._sp())
+        if code not in (0, 3, 8):
+            _lib.check(code, "batch_newton_step")
+        return norms, list(status)
 
     def condense(self):
         _lib.check(self.L.ddhdg_batch_condense(self._b, self._sp()), "batch_condense")

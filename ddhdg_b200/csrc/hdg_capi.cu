@@ -2184,8 +2184,21 @@ struct ddhdg_batch
   int                      sm_count             = 148;
   cudaStream_t             cap                  = nullptr;
   cudaGraphExec_t          g_c = nullptr, g_r = nullptr;
+  // Newton steps: norm words and side streams
+  static constexpr int     NS = 8;
+  DevBuf<unsigned long long> norms;
+  cudaStream_t             side[NS] = {};
+  cudaEvent_t              ev_fork = nullptr, ev_join[NS] = {};
   ~ddhdg_batch()
   {
+    for (auto &st : side)
+      if (st)
+        cudaStreamDestroy(st);
+    for (auto &e : ev_join)
+      if (e)
+        cudaEventDestroy(e);
+    if (ev_fork)
+      cudaEventDestroy(ev_fork);
     if (g_c)
       cudaGraphExecDestroy(g_c);
     if (g_r)
@@ -2558,6 +2571,115 @@ ddhdg_batch_reconstruct(ddhdg_batch *b, ddhdg_stream_t stream)
     if (!J.dtrace || !J.dcell)
       return fail(DDHDG_BAD_ARG, "a batch item has no update_trace / update_cell");
   return batch_run(b, (cudaStream_t)stream, true);
+}
+
+int
+ddhdg_batch_newton_step(ddhdg_batch *b, const double *alpha, double *norms_host, int *status_host,
+                        ddhdg_stream_t stream)
+{
+  if (!b || !alpha || !norms_host)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  for (const auto &J : b->jobs)
+    if (!J.dtrace || !J.dcell)
+      return fail(DDHDG_BAD_ARG, "a batch item has no update_trace / update_cell");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int    n = b->n;
+  int          r;
+  if (!b->ev_fork)
+    {
+      // each item's restricted trace solution lives in its context (the
+      // same buffer whatever batch the context is in, so that the context's
+      // trace-solve graph stays valid across batches)
+      for (int i = 0; i < n; ++i)
+        {
+          ddhdg_ctx *c = b->ctx[i];
+          Mode      &m = c->mode[b->thermo];
+          if (!m.built && (r = build_mode(c, b->thermo)))
+            return r;
+          if ((r = m.x.alloc(m.ndofs)))
+            return r;
+        }
+      if ((r = b->norms.alloc((size_t)4 * n)))
+        return r;
+      for (int k = 0; k < ddhdg_batch::NS; ++k)
+        {
+          CK(cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking));
+          CK(cudaEventCreateWithFlags(&b->ev_join[k], cudaEventDisableTiming));
+        }
+      CK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    }
+  for (int i = 0; i < n; ++i)
+    CK(cudaMemsetAsync(b->ctx[i]->status.p, 0, sizeof(int), s));
+  // 1) one launch: assembly + condensation of every item
+  if ((r = batch_run(b, s, false)))
+    return r;
+  // 2) every item's trace solve, on side streams so that they overlap
+  CK(cudaEventRecord(b->ev_fork, s));
+  const int used = std::min(n, ddhdg_batch::NS);
+  for (int k = 0; k < used; ++k)
+    CK(cudaStreamWaitEvent(b->side[k], b->ev_fork, 0));
+  for (int i = 0; i < n; ++i)
+    {
+      ddhdg_ctx     *c  = b->ctx[i];
+      Mode          &m  = c->mode[b->thermo];
+      const BatchJob &J = b->jobs[i];
+      cudaStream_t   ss = b->side[i % ddhdg_batch::NS];
+      NDSolver      *nd = nullptr;
+      if ((r = nd_solver(c, m, nd)))
+        return r;
+      std::string err;
+      if ((r = nd->solve(J.P.tt, J.P.rhs, J.P.dflag, J.P.dval, m.Nt, m.x.p, ss, c->sm_count, err, false)))
+        return fail(r, err);
+      const int64_t ntr = c->nfaces * 3 * c->nf;
+      expand_kernel<<<grid_for(c, ntr, 256), 256, 0, ss>>>(c->nfaces, c->nf, m.ncomp, m.comps[0], m.comps[1],
+                                                           m.comps[2], m.x.p, const_cast<double *>(J.dtrace));
+    }
+  for (int k = 0; k < used; ++k)
+    {
+      CK(cudaEventRecord(b->ev_join[k], b->side[k]));
+      CK(cudaStreamWaitEvent(s, b->ev_join[k], 0));
+    }
+  // 3) one launch: reconstruction of every item
+  if ((r = batch_run(b, s, true)))
+    return r;
+  // 4) norms before the update, then state += alpha (dcell, dtrace)
+  CK(cudaMemsetAsync(b->norms.p, 0, (size_t)4 * n * sizeof(unsigned long long), s));
+  for (int i = 0; i < n; ++i)
+    {
+      ddhdg_ctx     *c   = b->ctx[i];
+      const BatchJob &J  = b->jobs[i];
+      const int64_t  ncd = c->ncells * 3 * (c->dim + 1) * c->nb;
+      const int64_t  ntr = c->nfaces * 3 * c->nf;
+      absmax_kernel<<<grid_for(c, ncd, 256), 256, 0, s>>>(J.dcell, ncd, J.dtrace, ntr, J.P.cell_state, ncd,
+                                                          J.P.trace_state, ntr, b->norms.p + 4 * i);
+      axpy2_kernel<<<grid_for(c, ncd + ntr, 256), 256, 0, s>>>(ntr, const_cast<double *>(J.P.trace_state),
+                                                               J.dtrace, ncd,
+                                                               const_cast<double *>(J.P.cell_state), J.dcell,
+                                                               alpha[i]);
+    }
+  CK(cudaGetLastError());
+  std::vector<int> st(n, 0);
+  CK(cudaMemcpyAsync(norms_host, b->norms.p, (size_t)4 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  for (int i = 0; i < n; ++i)
+    CK(cudaMemcpyAsync(&st[i], b->ctx[i]->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  // singular fronts of the trace solves (their pivot status, read now)
+  int worst = DDHDG_OK;
+  for (int i = 0; i < n; ++i)
+    {
+      ddhdg_ctx  *c  = b->ctx[i];
+      NDSolver   *nd = nullptr;
+      std::string err;
+      if (nd_solver(c, c->mode[b->thermo], nd) == DDHDG_OK && nd->check_info(s, err) != DDHDG_OK)
+        st[i] = DDHDG_SOLVER_ERROR;
+      if (status_host)
+        status_host[i] = st[i];
+      if (st[i] && !worst)
+        worst = st[i];
+    }
+  if (worst)
+    return fail(worst, "a batch item had a singular local system or trace front (see the item statuses)");
+  return DDHDG_OK;
 }
 
 int

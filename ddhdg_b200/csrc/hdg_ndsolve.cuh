@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <utility>
@@ -1052,11 +1053,90 @@ namespace ddhdg
 
     int64_t front_bytes() const { return front_total_ * (int64_t)sizeof(double); }
 
-    // symbolic phase on the host: tree, fronts, maps and batches
+    // the plan's batches: {height, eliminated dofs, kept dofs, fronts, kind}
+    // with kind 0 fused, 1 small, 2 mid, 3 own LU + batched products, 4 big
+    std::vector<std::vector<int>>
+    batch_shapes() const
+    {
+      std::vector<std::vector<int>> out;
+      for (const auto &b : batches_)
+        out.push_back({b.height, b.nE, b.nK, (int)b.nodes.size(),
+                       b.fused ? 0 : b.small ? 1 : b.mid ? 2 : b.big ? 4 : 3});
+      return out;
+    }
+
+    // symbolic phase on the host: tree, fronts, maps and batches.  The plan
+    // depends on the mesh shape only, so plans are kept in a small process-
+    // wide cache: contexts of the same shape (the serving layer's requests,
+    // a bias sweep's solvers) reuse it instead of building it again (0.5 s
+    // on the host for 65 536 cells).
     int
     plan(const Mesh &M, std::string &err)
     {
       release();
+      {
+        std::lock_guard<std::mutex> lock(plan_cache_mutex());
+        for (auto &e : plan_cache())
+          if (same_mesh(e->M, M))
+            {
+              load_plan(*e);
+              return DDHDG_OK;
+            }
+      }
+      int r = plan_uncached(M, err);
+      if (r)
+        return r;
+      std::shared_ptr<PlanState> e(new PlanState);
+      save_plan(*e);
+      std::lock_guard<std::mutex> lock(plan_cache_mutex());
+      auto &c = plan_cache();
+      c.insert(c.begin(), std::move(e));
+      // at most 8 plans, and no more than 4 GB of host copies
+      size_t bytes = 0, keep = 0;
+      for (; keep < c.size() && keep < 8; ++keep)
+        {
+          bytes += c[keep]->bytes();
+          if (bytes > ((size_t)4 << 30) && keep > 0)
+            break;
+        }
+      c.resize(keep);
+      return DDHDG_OK;
+    }
+
+  private:
+    struct PlanState;
+    static bool
+    same_mesh(const Mesh &a, const Mesh &b)
+    {
+      if (a.dim != b.dim || a.ncells != b.ncells || a.nfaces != b.nfaces || a.F != b.F || a.nd != b.nd)
+        return false;
+      for (int i = 0; i < 3; ++i)
+        {
+          if (a.n[i] != b.n[i] || a.face_off[i] != b.face_off[i])
+            return false;
+          for (int j = 0; j < 3; ++j)
+            if (a.face_ext[i][j] != b.face_ext[i][j])
+              return false;
+        }
+      return true;
+    }
+    static std::mutex &
+    plan_cache_mutex()
+    {
+      static std::mutex mu;
+      return mu;
+    }
+    static std::vector<std::shared_ptr<PlanState>> &
+    plan_cache()
+    {
+      static std::vector<std::shared_ptr<PlanState>> c;
+      return c;
+    }
+
+  public:
+    int
+    plan_uncached(const Mesh &M, std::string &err)
+    {
       M_ = M;
       if (M.F > 6 || M.dim < 1 || M.dim > 3)
         return bad(err, "unsupported mesh for the nested-dissection solve");
@@ -1303,7 +1383,7 @@ namespace ddhdg
 
     int
     solve(const double *tt, const double *rhs, const int32_t *dflag, const double *dval, int Nt,
-          double *x, cudaStream_t s, int sm_count, std::string &err)
+          double *x, cudaStream_t s, int sm_count, std::string &err, bool check = true)
     {
       if (!built_)
         return bad(err, "nested-dissection solver not built");
@@ -1354,7 +1434,9 @@ namespace ddhdg
         }
       if (r)
         return r;
-      return check_info(s, err);
+      // check = false: the caller reads the per-front pivot status later
+      // (check_info), so that solves on several streams overlap
+      return check ? check_info(s, err) : DDHDG_OK;
     }
 
   private:
@@ -1509,6 +1591,7 @@ namespace ddhdg
       return DDHDG_OK;
     }
 
+  public:
     // singular fronts (outside any graph: a host read)
     int
     check_info(cudaStream_t s, std::string &err)
@@ -1523,6 +1606,8 @@ namespace ddhdg
           return bad(err, "global trace matrix is singular (zero pivot in a front)", DDHDG_SOLVER_ERROR);
       return DDHDG_OK;
     }
+
+  private:
 
     static constexpr int NSide = 8; // side streams for the large fronts
 
@@ -1793,6 +1878,71 @@ namespace ddhdg
       key_       = Key{};
       graphs_ok_ = true;
       built_ = false;
+    }
+
+    // a cached plan: the members that plan_uncached fills
+    struct PlanState
+    {
+      Mesh                 M;
+      std::vector<Node>    nodes;
+      std::vector<Batch>   batches;
+      std::vector<int64_t> cell_faces;
+      int                  root = -1, max_nK = 0;
+      int64_t              front_total = 0, piv_total = 0;
+      std::vector<int32_t> fdofs, emap;
+      std::vector<int64_t> leaf_off, ptr;
+      std::vector<uint8_t> pmask;
+      std::vector<NDAsm>   asm_;
+      std::vector<NDSol>   sol;
+      size_t
+      bytes() const
+      {
+        size_t b = cell_faces.size() * 8 + fdofs.size() * 4 + emap.size() * 4 + leaf_off.size() * 8 +
+                   ptr.size() * 8 + pmask.size() + asm_.size() * sizeof(NDAsm) + sol.size() * sizeof(NDSol);
+        for (const auto &n : nodes)
+          b += sizeof(Node) + n.dofs.size() * 4;
+        for (const auto &bt : batches)
+          b += sizeof(Batch) + bt.nodes.size() * 4;
+        return b;
+      }
+    };
+    void
+    save_plan(PlanState &e) const
+    {
+      e.M           = M_;
+      e.nodes       = nodes_;
+      e.batches     = batches_;
+      e.cell_faces  = cell_faces_;
+      e.root        = root_;
+      e.max_nK      = max_nK_;
+      e.front_total = front_total_;
+      e.piv_total   = piv_total_;
+      e.fdofs       = fdofs_h_;
+      e.emap        = emap_h_;
+      e.leaf_off    = leaf_off_h_;
+      e.ptr         = ptr_h_;
+      e.pmask       = pmask_h_;
+      e.asm_        = asm_h_;
+      e.sol         = sol_h_;
+    }
+    void
+    load_plan(const PlanState &e)
+    {
+      M_           = e.M;
+      nodes_       = e.nodes;
+      batches_     = e.batches;
+      cell_faces_  = e.cell_faces;
+      root_        = e.root;
+      max_nK_      = e.max_nK;
+      front_total_ = e.front_total;
+      piv_total_   = e.piv_total;
+      fdofs_h_     = e.fdofs;
+      emap_h_      = e.emap;
+      leaf_off_h_  = e.leaf_off;
+      ptr_h_       = e.ptr;
+      pmask_h_     = e.pmask;
+      asm_h_       = e.asm_;
+      sol_h_       = e.sol;
     }
 
     Mesh                 M_;

@@ -2,14 +2,19 @@
 
 Requests (a diode's dimension, mesh, degree and bias) arrive over time.  The
 server admits a request as soon as an in-flight slot and enough free device
-memory are available.  Every admitted request runs in its own host worker
-thread, with its own context and its own CUDA stream, so that the device work
-of the requests in flight overlaps; their Newton state stays on the device
-for the whole solve.  The C calls release the GIL, so the workers' host sides
-interleave as well.  Results do not depend on what else runs: every kernel is
-deterministic (no atomics with more than two contributions, no
-order-dependent reductions), so a request's fields are the same alone and in
-the mix.
+memory are available, and keeps its Newton state on the device for the whole
+solve.  ``DiodeServer`` batches at kernel level, step by step: every request
+in flight advances one Newton step per server step, the assembly and
+condensation of all requests in the same phase run as ONE batched launch
+(``ddhdg_batch_newton_step``), their trace solves overlap on side streams,
+and the reconstruction is one more launch; requests join at the next step
+after they arrive and leave when they converge (continuous batching).
+``ThreadedDiodeServer`` is the simpler form: one host thread, context and
+stream per request, overlapping only on the device.  Results do not depend on
+what else runs: every kernel is deterministic (no atomics with more than two
+contributions, no order-dependent reductions) and a device's results in a
+batched launch are bitwise those of its own launch, so a request's fields
+are the same alone and in the mix.
 
 A solve is: thermodynamic equilibrium (charge-neutral first guess, V-only
 Newton, density projection), then, for a nonzero bias, the contact
@@ -115,8 +120,8 @@ def solve_one(req: Request, device="cuda:0", keep_state=False, tol=1e-10, max_it
     return res.converged, it, g.ncells, state
 
 
-class DiodeServer:
-    """Continuous batching of diode solves on one GPU.
+class ThreadedDiodeServer:
+    """Concurrent diode solves on one GPU, one host thread per request.
 
     max_inflight: requests on the device at once (slots).
     hbm_reserve: bytes of device memory left free for everything else.
@@ -239,3 +244,159 @@ def latency_stats(results, wall):
             "mean_s": float(lat.mean()), "solves_per_s": len(results) / wall,
             "cells_per_s": sum(r.cells for r in results) / wall,
             "converged": int(sum(r.converged for r in results)), "requests": len(results)}
+
+
+class _Active:
+    """A request in flight: its solver, phase and per-phase batch buffers."""
+
+    def __init__(self, req, est, start):
+        self.req, self.est, self.start = req, est, start
+        self.solver = None
+        self.phase = "eq"  # thermodynamic equilibrium, then the biased solve
+        self.it = 0        # iterations of the current phase
+        self.total_it = 0
+        self.buffers = {}
+
+
+class DiodeServer(ThreadedDiodeServer):
+    """Continuous batching of diode solves on one GPU, at kernel level.
+
+    Every server step advances each request in flight by one Newton step:
+    one batched condensation launch over all requests of a phase, their trace
+    solves overlapped on side streams, one batched reconstruction launch and
+    the damped updates (``CondenseBatch.newton_step``).  The loop is
+    ``private_run`` (src/np_solver.cpp:1452-1561) per request: the stopping
+    rule on the update and state norms and the damping are the solver's.
+    Arrivals join at the next step once a slot and their device memory are
+    free; converged requests leave.  Memory admission as in
+    ``ThreadedDiodeServer``."""
+
+    def __init__(self, max_inflight=16, hbm_reserve=4 << 30, hbm_limit=None, device="cuda:0",
+                 keep_states=False, mem_info=None, tol=1e-10, max_it=50):
+        super().__init__(max_inflight, hbm_reserve, hbm_limit, device, keep_states, mem_info)
+        self.tol = tol
+        self.max_it = max_it
+        self.steps = 0
+        self.peak_batch = 0
+
+    def _start_request(self, a):
+        from . import workloads
+        from .solver import NPSolver
+
+        req = a.req
+        pb, prm, adim = workloads.diode(dim=req.dim, m=req.m, k=req.k)
+        prm.consistent_drift_jacobian = True
+        prm.consistent_recombination_jacobian = True
+        g = NPSolver(pb, prm, adim, device=self.device)
+        g.compute_local_charge_neutrality()
+        a.solver, a.problem = g, pb
+        nl = prm.nonlinear_parameters
+        a.eq_tol = (nl.absolute_tolerance, nl.relative_tolerance, nl.max_number_of_iterations)
+        a.alpha = nl.alpha
+
+    def _finish_phase(self, a):
+        """Equilibrium done: densities from the equilibrium potential, then
+        the contact conditions of the bias (or the end of the solve)."""
+        from . import _lib, workloads
+
+        g = a.solver
+        a.total_it += a.it
+        a.it = 0
+        if a.phase == "eq":
+            for c in (1, 2):
+                _lib.check(g.L.ddhdg_project_density(g._ctx, c, 0.0, g.cell_state.data_ptr(),
+                                                     g.trace_state.data_ptr(), g._sp()), "project_density")
+            if a.req.bias != 0.0:
+                workloads.set_bias(a.problem, a.req.bias)
+                g.update_boundary_tables()
+                a.phase = "bias"
+                return False
+        return True
+
+    def run(self, requests):
+        import torch
+
+        from .batch import CondenseBatch
+
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        results, errors = {}, []
+        active = []
+        committed = 0
+        batches = {}  # (phase, dim) -> (member ids, CondenseBatch)
+        self._start_accounting()
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(reqs) or active:
+            now = time.perf_counter() - t0
+            # admission at the step boundary
+            while i < len(reqs) and reqs[i].arrival <= now and len(active) < self.max_inflight:
+                req = reqs[i]
+                est = memory_estimate(req.dim, req.m, req.k)
+                if not self.admissible(est, committed):
+                    if not active:
+                        errors.append((req.rid, "does not fit in device memory"))
+                        i += 1
+                        continue
+                    break
+                a = _Active(req, est, time.perf_counter() - t0)
+                self._start_request(a)
+                active.append(a)
+                committed += est
+                i += 1
+                self.peak_inflight = max(self.peak_inflight, len(active))
+                self.peak_committed = max(self.peak_committed, committed)
+            if not active:
+                if i < len(reqs):
+                    time.sleep(max(0.0, min(reqs[i].arrival - (time.perf_counter() - t0), 0.05)))
+                continue
+            self.steps += 1
+            done = []
+            # one batch per (phase, dimension): a batched launch holds
+            # devices of one dimension and one mode
+            groups = {}
+            for a in active:
+                groups.setdefault((a.phase, a.req.dim), []).append(a)
+            for bk in sorted(groups):
+                phase, group = bk[0], groups[bk]
+                key = tuple(id(a) for a in group)
+                if bk not in batches or batches[bk][0] != key:
+                    if bk in batches:
+                        batches[bk][1].close()
+                    bufs = []
+                    for a in group:
+                        if phase not in a.buffers:
+                            a.buffers[phase] = CondenseBatch.buffers_for(a.solver, thermo=(phase == "eq"))
+                        bufs.append(a.buffers[phase])
+                    batches[bk] = (key, CondenseBatch([a.solver for a in group], thermo=(phase == "eq"),
+                                                      buffers=bufs))
+                self.peak_batch = max(self.peak_batch, len(group))
+                norms, status = batches[bk][1].newton_step([a.alpha for a in group])
+                for a, nrm, st in zip(group, norms, status):
+                    a.it += 1
+                    upd, cur = max(nrm[0], nrm[1]), max(nrm[2], nrm[3])
+                    abs_tol, rel_tol, max_it = a.eq_tol if phase == "eq" else (self.tol, self.tol, self.max_it)
+                    if st or not math.isfinite(upd):
+                        errors.append((a.req.rid, f"Newton failed in phase {phase} (status {st})"))
+                        done.append((a, False))
+                    elif upd < abs_tol or upd < rel_tol * cur:
+                        if self._finish_phase(a):
+                            done.append((a, True))
+                    elif a.it >= max_it:
+                        a.total_it += a.it
+                        done.append((a, False))
+            for a, conv in done:
+                active.remove(a)
+                committed -= a.est
+                g = a.solver
+                torch.cuda.synchronize(self.device)
+                finish = time.perf_counter() - t0
+                state = (g.get_cell_state().copy(), g.get_trace_state().copy()) if self.keep_states else None
+                results[a.req.rid] = Result(a.req.rid, a.req.arrival, a.start, finish, a.total_it, conv,
+                                            g.ncells, state)
+                a.solver = None
+                a.buffers = {}
+        for _, b in batches.values():
+            b.close()
+        if errors:
+            raise RuntimeError(f"requests failed: {errors}")
+        return [results[r.rid] for r in requests]

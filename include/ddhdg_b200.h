@@ -354,7 +354,7 @@ typedef struct ddhdg_batch_item
   double       *tt, *rhs;                 /* condensation outputs, as in  */
   int32_t      *dflag;                    /* ddhdg_assemble_condense      */
   double       *dval;
-  const double *update_trace; /* reconstruction input (or NULL)  */
+  double       *update_trace; /* reconstruction input (or NULL); written by ddhdg_batch_newton_step */
   double       *update_cell;  /* reconstruction output (or NULL) */
 } ddhdg_batch_item;
 
@@ -363,6 +363,18 @@ int ddhdg_batch_create(const ddhdg_batch_item *items, int nitems, int thermo_eq,
 int ddhdg_batch_destroy(ddhdg_batch *batch);
 int ddhdg_batch_condense(ddhdg_batch *batch, ddhdg_stream_t stream);
 int ddhdg_batch_reconstruct(ddhdg_batch *batch, ddhdg_stream_t stream);
+/* One Newton step of private_run (src/np_solver.cpp:1470-1555) for every item:
+ * the batched condensation, every item's trace solve (ddhdg_solve_condensed,
+ * on side streams forked from `stream`, so that they overlap), the trace
+ * update expanded into update_trace, the batched reconstruction, and
+ * state += alpha[i] (update_cell, update_trace) in place.  norms_host[4 i ..]
+ * (host) receives max |update_cell|, max |update_trace|, max |cell_state|,
+ * max |trace_state| of item i before its update (the stopping rule of
+ * private_run is the caller's); status_host[i] (host, may be NULL) the item's
+ * status (DDHDG_SINGULAR_PIVOT, DDHDG_SOLVER_ERROR or 0).  Returns when the
+ * step has completed. */
+int ddhdg_batch_newton_step(ddhdg_batch *batch, const double *alpha, double *norms_host,
+                            int *status_host, ddhdg_stream_t stream);
 /* Tile shape: cells per tile for degrees 1, 2, 3 (cells_per_tile[3]) and
  * CTAs per SM.  ddhdg_batch_autotune picks them by timing the batch's own
  * condensation launch (coordinate search, best of `reps` launches per

@@ -1,6 +1,8 @@
 """Serving (continuous batching of diode solves on one GPU): every request's
-fields are the same alone and in the mix, requests really overlap, and the
-memory admission holds requests back when the device is full."""
+fields are the same alone and in the mix, requests really overlap (the
+batched server condenses all of them in one launch per step), the batched
+and the thread-per-request servers give the same bits, and the memory
+admission holds requests back when the device is full."""
 
 import numpy as np
 import pytest
@@ -22,8 +24,8 @@ def test_results_are_the_same_alone_and_in_the_mix():
     if not torch.cuda.is_available():
         pytest.skip("needs a GPU")
     reqs = _requests()
-    alone = serving.DiodeServer(max_inflight=1, keep_states=True).run(reqs)
-    mixed_server = serving.DiodeServer(max_inflight=4, keep_states=True)
+    alone = serving.ThreadedDiodeServer(max_inflight=1, keep_states=True).run(reqs)
+    mixed_server = serving.ThreadedDiodeServer(max_inflight=4, keep_states=True)
     mixed = mixed_server.run(reqs)
     assert mixed_server.peak_inflight > 1
     for a, b in zip(alone, mixed):
@@ -40,7 +42,7 @@ def test_memory_admission_limits_the_requests_in_flight():
     reqs = _requests()
     biggest = max(serving.memory_estimate(r.dim, r.m, r.k) for r in reqs)
     limit = 2 * biggest
-    server = serving.DiodeServer(max_inflight=8, hbm_reserve=0, hbm_limit=limit)
+    server = serving.ThreadedDiodeServer(max_inflight=8, hbm_reserve=0, hbm_limit=limit)
     res = server.run(reqs)
     assert all(r.converged for r in res)
     assert server.peak_committed <= limit
@@ -48,3 +50,36 @@ def test_memory_admission_limits_the_requests_in_flight():
     assert server.peak_committed < total  # some requests had to wait
     stats = serving.latency_stats(res, max(r.finish for r in res))
     assert stats["p99_s"] >= stats["p50_s"] > 0
+
+
+def test_batched_server_same_alone_in_the_mix_and_as_the_threaded_server():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    reqs = _requests()
+    alone = serving.DiodeServer(max_inflight=1, keep_states=True).run(reqs)
+    server = serving.DiodeServer(max_inflight=8, keep_states=True)
+    mixed = server.run(reqs)
+    assert server.peak_batch > 1  # several requests in one batched launch
+    threaded = serving.ThreadedDiodeServer(max_inflight=1, keep_states=True).run(reqs)
+    for a, b, c in zip(alone, mixed, threaded):
+        assert a.converged and b.converged and c.converged
+        assert a.iterations == b.iterations == c.iterations, (a.rid, a.iterations, b.iterations, c.iterations)
+        for x, y, z in zip(a.state, b.state, c.state):
+            assert np.array_equal(x, y), a.rid
+            assert np.array_equal(x, z), a.rid
+
+
+def test_batched_server_memory_admission():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    reqs = _requests()
+    biggest = max(serving.memory_estimate(r.dim, r.m, r.k) for r in reqs)
+    limit = 2 * biggest
+    server = serving.DiodeServer(max_inflight=8, hbm_reserve=0, hbm_limit=limit)
+    res = server.run(reqs)
+    assert all(r.converged for r in res)
+    assert server.peak_committed <= limit
+    total = sum(serving.memory_estimate(r.dim, r.m, r.k) for r in reqs)
+    assert server.peak_committed < total
