@@ -21,11 +21,16 @@
 //                           Schur update); above the leaves, while the front
 //                           fits, it is also assembled in shared memory
 //   37..72                  a CTA per front for the LU and W, the Schur update
-//                           as a batched cuBLAS GEMM
-//   up to 383               own LU, a CTA per front (all fronts at once),
-//                           batched cuBLAS triangular solves and GEMMs
-//   >= 384 (few fronts)     cuSOLVER LU per front, cuBLAS triangular solves
-//                           and GEMM, fronts spread over side streams
+//                           on the FP64 tensor path for all fronts at once
+//                           (nd_gemm_kernel, hdg_ndblas.cuh)
+//   up to 383               own LU, a CTA per front (all fronts at once); W by
+//                           triangular solves with inverted 32 x 32 diagonal
+//                           blocks and the Schur update, both on the tensor
+//                           path for all fronts at once (hdg_ndblas.cuh)
+//   >= 384 (few fronts)     cuSOLVER LU per front on side streams, then W and
+//                           the Schur update as above for all fronts at once
+// (DDHDG_ND_LIBRARY_PRODUCTS=1 puts W and the Schur updates back on cuBLAS,
+// for comparison.)
 // The numeric sequence is captured in a CUDA graph on the second call with
 // the same buffers and replayed afterwards.  Before the factorisation the
 // rows are equilibrated: row g is scaled by 1 / max |row g| over the cells
@@ -38,6 +43,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -46,6 +52,7 @@
 #include <vector>
 
 #include "../../include/ddhdg_b200.h"
+#include "hdg_ndblas.cuh"
 
 namespace ddhdg
 {
@@ -1303,6 +1310,17 @@ namespace ddhdg
       // one info per node, plus a sink for the solves' parameter status
       if ((r = dmalloc(d_info_, (nodes_.size() + 1) * sizeof(int), err)))
         return r;
+      // inverted diagonal blocks of the triangular solves (largest batch)
+      {
+        int64_t tinv = 1;
+        for (const auto &b : batches_)
+          if (b.nE > 0 && !b.small && !b.fused && !b.mid)
+            tinv = std::max<int64_t>(tinv, (int64_t)b.nodes.size() * ((b.nE + NDTB - 1) / NDTB) * 2 * NDTB * NDTB);
+        if ((r = dmalloc(d_tinv_, tinv * sizeof(double), err)))
+          return r;
+        const char *e = getenv("DDHDG_ND_LIBRARY_PRODUCTS");
+        own_blas_     = !(e && e[0] == '1');
+      }
       if ((r = upload(d_fdofs_, fdofs_h_, err)) || (r = upload(d_emap_, emap_h_, err)) ||
           (r = upload(d_leaf_off_, leaf_off_h_, err)) || (r = upload(d_pmask_, pmask_h_, err)) ||
           (r = upload(d_cell_faces_, cell_faces_, err)) || (r = upload(d_asm_, asm_h_, err)) ||
@@ -1531,13 +1549,9 @@ namespace ddhdg
                 {
                   nd_mid_front_kernel<<<nb, NDMidTPB, nd_mid_smem(b.nE), s>>>(b.nE, b.nK, d_sol_ + b.sol_off,
                                                                              inf, d_fronts_);
-                  if (b.nK > 0)
-                    {
-                      const double mone = -1., one = 1.;
-                      if (cublasDgemmBatched(blas_, CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE, &mone,
-                                             pKE, nF, pEK, nF, &one, pKK, nF, nb) != CUBLAS_STATUS_SUCCESS)
-                        return bad(err, "cublasDgemmBatched failed", DDHDG_SOLVER_ERROR);
-                    }
+                  int r;
+                  if (b.nK > 0 && (r = schur_update(b, pKE, pEK, pKK, s, err)))
+                    return r;
                   info_base += nb;
                   continue;
                 }
@@ -1555,21 +1569,11 @@ namespace ddhdg
                 nd_rowperm_kernel<<<g2, 256, b.nE * sizeof(double), s>>>(b.nE, nF, d_sol_ + b.sol_off,
                                                                          perm, d_fronts_);
               }
-              const double one_ = 1.;
-              if (cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                                     CUBLAS_DIAG_UNIT, b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF,
-                                     nb) != CUBLAS_STATUS_SUCCESS ||
-                  cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
-                                     CUBLAS_DIAG_NON_UNIT, b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF,
-                                     nb) != CUBLAS_STATUS_SUCCESS)
-                return bad(err, "cublasDtrsmBatched failed", DDHDG_SOLVER_ERROR);
-              if (b.nK > 0)
-                {
-                  const double mone = -1., one = 1.;
-                  if (cublasDgemmBatched(blas_, CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE, &mone,
-                                         pKE, nF, pEK, nF, &one, pKK, nF, nb) != CUBLAS_STATUS_SUCCESS)
-                    return bad(err, "cublasDgemmBatched failed", DDHDG_SOLVER_ERROR);
-                }
+              int r;
+              if ((r = solve_w(b, pEE, pEK, s, err)))
+                return r;
+              if (b.nK > 0 && (r = schur_update(b, pKE, pEK, pKK, s, err)))
+                return r;
             }
           info_base += nb;
         }
@@ -1669,6 +1673,8 @@ namespace ddhdg
           const dim3 g2(1, (b.nK + 1 + NDPermCols - 1) / NDPermCols);
           nd_rowperm_kernel<<<g2, 256, b.nE * sizeof(double), ss>>>(b.nE, nF, d_sol_ + b.sol_off + q,
                                                                     pm, d_fronts_);
+          if (own_blas_)
+            continue; // W and the Schur update for all fronts at once, below
           double *B = Fq + (int64_t)b.nE * nF;
           if (cublasDtrsm(side_blas_[k], CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
                           CUBLAS_DIAG_UNIT, b.nE, b.nK + 1, &one, Fq, nF, B, nF) != CUBLAS_STATUS_SUCCESS ||
@@ -1684,6 +1690,59 @@ namespace ddhdg
         if (cudaEventRecord(ev_join_[k], side_[k]) != cudaSuccess ||
             cudaStreamWaitEvent(s, ev_join_[k], 0) != cudaSuccess)
           return bad(err, "stream join failed", DDHDG_CUDA_ERROR);
+      if (own_blas_)
+        {
+          double **pEE = d_ptr_ + b.ptr_off, **pEK = pEE + nb, **pKE = pEK + nb, **pKK = pKE + nb;
+          int      r;
+          if ((r = solve_w(b, pEE, pEK, s, err)))
+            return r;
+          if (b.nK > 0 && (r = schur_update(b, pKE, pEK, pKK, s, err)))
+            return r;
+        }
+      return DDHDG_OK;
+    }
+
+    // W = U^-1 L^-1 [F_EK | r_E] for every front of a batch (after the row
+    // permutation), by the tensor-path kernels or by batched cuBLAS
+    int
+    solve_w(const Batch &b, double **pEE, double **pEK, cudaStream_t s, std::string &err)
+    {
+      const int nF = b.nE + b.nK;
+      const int nb = (int)b.nodes.size();
+      if (own_blas_)
+        {
+          const int nblk = (b.nE + NDTB - 1) / NDTB;
+          nd_trinv_kernel<<<dim3(nblk, nb), 64, 0, s>>>(b.nE, nF, pEE, d_tinv_);
+          nd_trsm_kernel<<<dim3((b.nK + 1 + NDTB - 1) / NDTB, nb), 128, 0, s>>>(b.nE, b.nK + 1, nF, pEE, pEK,
+                                                                                 d_tinv_);
+          return DDHDG_OK;
+        }
+      const double one_ = 1.;
+      if (cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT,
+                             b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF, nb) != CUBLAS_STATUS_SUCCESS ||
+          cublasDtrsmBatched(blas_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                             CUBLAS_DIAG_NON_UNIT, b.nE, b.nK + 1, &one_, pEE, nF, pEK, nF,
+                             nb) != CUBLAS_STATUS_SUCCESS)
+        return bad(err, "cublasDtrsmBatched failed", DDHDG_SOLVER_ERROR);
+      return DDHDG_OK;
+    }
+
+    // F_KK -= F_KE W for every front of a batch
+    int
+    schur_update(const Batch &b, double **pKE, double **pEK, double **pKK, cudaStream_t s, std::string &err)
+    {
+      const int nF = b.nE + b.nK;
+      const int nb = (int)b.nodes.size();
+      if (own_blas_)
+        {
+          const int tiles = ((b.nK + NDGM - 1) / NDGM) * ((b.nK + 1 + NDGN - 1) / NDGN);
+          nd_gemm_kernel<<<dim3(tiles, nb), 128, 0, s>>>(b.nK, b.nK + 1, b.nE, nF, pKE, pEK, pKK);
+          return DDHDG_OK;
+        }
+      const double mone = -1., one = 1.;
+      if (cublasDgemmBatched(blas_, CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE, &mone, pKE, nF, pEK, nF,
+                             &one, pKK, nF, nb) != CUBLAS_STATUS_SUCCESS)
+        return bad(err, "cublasDgemmBatched failed", DDHDG_SOLVER_ERROR);
       return DDHDG_OK;
     }
 
@@ -1961,6 +2020,8 @@ namespace ddhdg
     // device
     std::vector<void *> allocs_;
     double             *d_fronts_ = nullptr, *d_dscale_ = nullptr, *d_work_ = nullptr;
+    double             *d_tinv_   = nullptr; // inverted diagonal blocks of the triangular solves
+    bool                own_blas_ = true;    // tensor-path kernels for W and the Schur updates
     double            **d_ptr_    = nullptr;
     int                *d_piv_ = nullptr, *d_perm_ = nullptr, *d_info_ = nullptr;
     int32_t            *d_fdofs_ = nullptr, *d_emap_ = nullptr;
