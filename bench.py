@@ -622,8 +622,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=4.0, help="arrivals per second")
     ap.add_argument("--serve-3d-min", type=int, default=16)
-    ap.add_argument("--serve-3d-max", type=int, default=24,
-                    help="largest 3D mesh of the stream (the nested-dissection fronts grow as m^5 in 3D)")
+    ap.add_argument("--serve-3d-max", type=int, default=32,
+                    help="largest 3D mesh of the stream (the nested-dissection fronts grow as m^4.1 in 3D)")
     ap.add_argument("--bias-sweep", action="store_true",
                     help="time the warm-started 0..0.8 V sweep (17 points) instead of the step")
     ap.add_argument("--mixed", action="store_true",

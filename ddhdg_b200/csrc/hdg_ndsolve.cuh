@@ -1709,7 +1709,11 @@ namespace ddhdg
     {
       const int nF = b.nE + b.nK;
       const int nb = (int)b.nodes.size();
-      if (own_blas_)
+      // each CTA of nd_trsm_kernel sweeps the whole column of blocks of its
+      // 32 right-hand sides: worth it while there are enough of them (not
+      // for the root's single column, nor for the largest 3D fronts)
+      const int ntiles = (b.nK + 1 + NDTB - 1) / NDTB;
+      if (own_blas_ && (int64_t)ntiles * nb >= 64 && b.nE <= 1152)
         {
           const int nblk = (b.nE + NDTB - 1) / NDTB;
           nd_trinv_kernel<<<dim3(nblk, nb), 64, 0, s>>>(b.nE, nF, pEE, d_tinv_);

@@ -61,8 +61,9 @@ class Result:
 def memory_estimate(dim: int, m: int, k: int) -> int:
     """Device bytes of one solve: states, condensed blocks, the Y cache and
     the fronts of the nested-dissection trace solve (the fronts dominate;
-    per cell about 320 nd^2 log2(m) bytes in 2D and 40 nd^2 m^2 in 3D, nd the
-    trace dofs per face, fitted to the solver's own plans and rounded up)."""
+    per cell about 320 nd^2 log2(m) bytes in 2D, and about m^4.1 in all in
+    3D, nd the trace dofs per face, fitted to the solver's own plans and
+    rounded up)."""
     nb = (k + 1) ** dim
     nf = (k + 1) ** (dim - 1)
     cells = m ** dim
@@ -75,7 +76,9 @@ def memory_estimate(dim: int, m: int, k: int) -> int:
     elif dim == 2:
         fronts = 320 * nd * nd * max(math.log2(m), 1.0) * cells
     else:
-        fronts = 40 * nd * nd * m * m * cells
+        # the solver's plans at degree 1: 5.5 GB at 16^3, 29.9 GB at 24^3,
+        # 94.9 GB at 32^3 (about m^4.1), 10 % over
+        fronts = 1.1 * 5.5e9 * (m / 16.0) ** 4.1 * (nd / 12.0) ** 2
     return int(per_cell * cells + fronts + (64 << 20))
 
 
