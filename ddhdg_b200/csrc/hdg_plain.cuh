@@ -789,20 +789,23 @@ namespace ddhdg
                 singular = true;
                 break;
               }
+            // a thread per column: row swap and rank-1 update of its own
+            // columns (the columns left of k are eliminated and not needed)
             if (p != k)
-              for (int j = tid; j < ncols; j += T)
+              for (int jj = k + tid; jj < ncols; jj += T)
                 {
-                  const double t  = A[k * ldA + j];
-                  A[k * ldA + j]  = A[p * ldA + j];
-                  A[p * ldA + j]  = t;
+                  const double t  = A[k * ldA + jj];
+                  A[k * ldA + jj] = A[p * ldA + jj];
+                  A[p * ldA + jj] = t;
                 }
             __syncthreads();
             const double inv = 1. / A[k * ldA + k];
-            const int    nr  = Nc - 1 - k, nc_ = ncols - 1 - k;
-            for (int idx = tid; idx < nr * nc_; idx += T)
+            for (int jj = k + 1 + tid; jj < ncols; jj += T)
               {
-                const int i = k + 1 + idx / nc_, j = k + 1 + idx % nc_;
-                A[i * ldA + j] -= A[i * ldA + k] * inv * A[k * ldA + j];
+                const double u = A[k * ldA + jj] * inv;
+                if (u != 0.)
+                  for (int ii = k + 1; ii < Nc; ++ii)
+                    A[ii * ldA + jj] -= A[ii * ldA + k] * u;
               }
             __syncthreads();
           }
@@ -813,23 +816,17 @@ namespace ddhdg
             __syncthreads();
             continue;
           }
-        // back substitution U X = Y for the right-hand-side columns: the
-        // step for row k updates the rows above it with row k unnormalised
-        for (int k = Nc - 1; k > 0; --k)
-          {
-            const double inv = 1. / A[k * ldA + k];
-            for (int idx = tid; idx < k * NR; idx += T)
-              {
-                const int i = idx / NR, j = Nc + idx % NR;
-                A[i * ldA + j] -= A[i * ldA + k] * inv * A[k * ldA + j];
-              }
-            __syncthreads();
-          }
-        for (int idx = tid; idx < Nc * NR; idx += T)
-          {
-            const int i = idx / NR, j = Nc + idx % NR;
-            A[i * ldA + j] /= A[i * ldA + i];
-          }
+        // back substitution U X = Y: a thread per right-hand-side column,
+        // reading only U (no barrier between the steps)
+        for (int jj = Nc + tid; jj < ncols; jj += T)
+          for (int kk = Nc - 1; kk >= 0; --kk)
+            {
+              const double x = A[kk * ldA + jj] / A[kk * ldA + kk];
+              A[kk * ldA + jj] = x;
+              if (x != 0.)
+                for (int ii = 0; ii < kk; ++ii)
+                  A[ii * ldA + jj] -= A[ii * ldA + kk] * x;
+            }
         __syncthreads();
 
         if (recon)
