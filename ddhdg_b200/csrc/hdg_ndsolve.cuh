@@ -21,16 +21,15 @@
 //                           Schur update); above the leaves, while the front
 //                           fits, it is also assembled in shared memory
 //   37..72                  a CTA per front for the LU and W, the Schur update
-//                           on the FP64 tensor path for all fronts at once
-//                           (nd_gemm_kernel, hdg_ndblas.cuh)
-//   up to 383               own LU, a CTA per front (all fronts at once); W by
-//                           triangular solves with inverted 32 x 32 diagonal
-//                           blocks and the Schur update, both on the tensor
-//                           path for all fronts at once (hdg_ndblas.cuh)
-//   >= 384 (few fronts)     cuSOLVER LU per front on side streams, then W and
-//                           the Schur update as above for all fronts at once
-// (DDHDG_ND_LIBRARY_PRODUCTS=1 puts W and the Schur updates back on cuBLAS,
-// for comparison.)
+//                           as a batched GEMM
+//   up to 383               own LU, a CTA per front (all fronts at once), then
+//                           batched triangular solves and GEMMs
+//   >= 384 (few fronts)     cuSOLVER LU per front on side streams, triangular
+//                           solves and GEMM per front
+// By default W and the Schur updates of these fronts use cuBLAS (batched or
+// per front); DDHDG_ND_OWN_PRODUCTS=1 switches them to the tensor-path
+// kernels of hdg_ndblas.cuh (measured slower on the 256 x 256 degree-2
+// diode: 100 against 88 ms per solve).
 // The numeric sequence is captured in a CUDA graph on the second call with
 // the same buffers and replayed afterwards.  Before the factorisation the
 // rows are equilibrated: row g is scaled by 1 / max |row g| over the cells
@@ -1318,8 +1317,8 @@ namespace ddhdg
             tinv = std::max<int64_t>(tinv, (int64_t)b.nodes.size() * ((b.nE + NDTB - 1) / NDTB) * 2 * NDTB * NDTB);
         if ((r = dmalloc(d_tinv_, tinv * sizeof(double), err)))
           return r;
-        const char *e = getenv("DDHDG_ND_LIBRARY_PRODUCTS");
-        own_blas_     = !(e && e[0] == '1');
+        const char *e = getenv("DDHDG_ND_OWN_PRODUCTS");
+        own_blas_     = e && e[0] == '1';
       }
       if ((r = upload(d_fdofs_, fdofs_h_, err)) || (r = upload(d_emap_, emap_h_, err)) ||
           (r = upload(d_leaf_off_, leaf_off_h_, err)) || (r = upload(d_pmask_, pmask_h_, err)) ||

@@ -71,6 +71,8 @@ def memory_estimate(dim: int, m: int, k: int) -> int:
     Ns = 3 * nb
     nd = 3 * nf
     per_cell = 8 * (3 * (dim + 1) * nb * 3 + Nt * Nt + 3 * Nt + Ns * (1 + Nt))
+    # the fronts of the full system, plus those of the equilibrium (V only,
+    # (1/3)^2 of them), which stay allocated for the rest of the solve
     if dim == 1:
         fronts = 64 * nd * nd * cells
     elif dim == 2:
@@ -79,7 +81,9 @@ def memory_estimate(dim: int, m: int, k: int) -> int:
         # the solver's plans at degree 1: 5.5 GB at 16^3, 29.9 GB at 24^3,
         # 94.9 GB at 32^3 (about m^4.1), 10 % over
         fronts = 1.1 * 5.5e9 * (m / 16.0) ** 4.1 * (nd / 12.0) ** 2
-    return int(per_cell * cells + fronts + (64 << 20))
+    fronts *= 1.0 + 1.0 / 9.0
+    # two sets of per-cell buffers (equilibrium and biased phases)
+    return int(2 * per_cell * cells + fronts + (64 << 20))
 
 
 def poisson_requests(n: int, rate: float, seed: int, sizes_2d=(32, 256), sizes_3d=(8, 16),
@@ -398,6 +402,13 @@ class DiodeServer(ThreadedDiodeServer):
                                             g.ncells, state)
                 a.solver = None
                 a.buffers = {}
+            if done:
+                # the batches held the finished requests' buffers; hand the
+                # memory back to the device (the trace solver allocates
+                # outside torch's cache)
+                for bk in [bk for bk, (key, _) in batches.items() if any(id(a) in key for a, _ in done)]:
+                    batches.pop(bk)[1].close()
+                torch.cuda.empty_cache()
         for _, b in batches.values():
             b.close()
         if errors:

@@ -68,6 +68,7 @@ def test_full_size_solve_and_newton():
     assert g.compute_thermodynamic_equilibrium().converged
     workloads.set_bias(pb, 0.3)
     g.update_boundary_tables()
+    start = (g.get_cell_state(), g.get_trace_state())
     # 1) the trace solve at full size
     g.assemble_system()
     xs = g.get_linear_system_solution_vector()
@@ -93,6 +94,15 @@ def test_full_size_solve_and_newton():
     o = OracleSolver(pb, prm, adim)
     sel = _sample_cells(256)
     assert sel.size >= 1024
+    # the converged fields solve the oracle's equations: its condensed
+    # residual on the sample is 1e8 times below the one at the start state
+    o.cell_state[:], o.trace_state[:] = start
+    _, g_start = o.condense_accurate(cells=sel)
+    o.cell_state[:] = g.get_cell_state()
+    o.trace_state[:] = g.get_trace_state()
+    _, g_conv = o.condense_accurate(cells=sel)
+    print(f"oracle residual on the sample: start {np.abs(g_start).max():.3e}, converged {np.abs(g_conv).max():.3e}")
+    assert np.abs(g_conv).max() <= 1e-8 * np.abs(g_start).max()
     rng = np.random.default_rng(21)
     for perturbed in (False, True):
         cs, ts = g.get_cell_state(), g.get_trace_state()
@@ -150,3 +160,17 @@ def test_full_size_mixed_newton_matches_fp64():
     print(f"256x256 k=2, 0.3 V: FP64 {r64.iterations} iterations, mixed {rm.iterations}; "
           f"final field difference {err:.2e}")
     assert err < 1e-8, err
+    # the mixed result against the oracle's own equations (FP64): its
+    # condensed residual on a sample of cells is 1e8 times below the start's
+    from oracle.oracle import OracleSolver
+    from tests.test_gpu_fullsize import _sample_cells as sample
+
+    o = OracleSolver(pbm, prmm, adimm)
+    sel = sample(256, n_interior=512)
+    o.cell_state[:], o.trace_state[:] = start
+    _, g_start = o.condense_accurate(cells=sel)
+    o.cell_state[:], o.trace_state[:] = c32, t32
+    _, g_conv = o.condense_accurate(cells=sel)
+    print(f"oracle residual at the mixed solution: start {np.abs(g_start).max():.3e}, "
+          f"converged {np.abs(g_conv).max():.3e}")
+    assert np.abs(g_conv).max() <= 1e-8 * np.abs(g_start).max()
