@@ -101,8 +101,9 @@ def fp64_peak_tflops(dev):
 # the 128 x 128 mesh of the same diode and scaled to a launch by the cells it
 # processes.  The figure belongs to one version of the kernel source: it is
 # reported only while the sha256 of hdg_condense3.cuh matches, else null.
-TRAFFIC = {"bytes_per_cell": 16806, "kernel_source": "ddhdg_b200/csrc/hdg_condense3.cuh",
-           "kernel_sha256": None}
+# Capture: 14 802 944 bytes read + 258 037 760 written for 16 384 cells.
+TRAFFIC = {"bytes_per_cell": 16653, "kernel_source": "ddhdg_b200/csrc/hdg_condense3.cuh",
+           "kernel_sha256": "d5384f79822f7dbd1d6ae0f683097c80fc9b3229c9cff646f9c20c7abf059b49"}
 
 
 def traffic_bytes_per_cell():
@@ -267,10 +268,11 @@ def run_serve(args):
 
     torch.cuda.init()
     # warm the library and the kernels once (not part of the stream)
-    serving.solve_one(serving.Request(-1, 2, 32, 1, 0.1, 0.0))
+    serving.solve_one(serving.Request(-1, 2, 32, 1, 0.1, 0.0), mixed=args.serve_precision == "mixed")
     reqs = serving.poisson_requests(args.serve_requests, args.serve_rate, seed=2024,
                                     sizes_3d=(args.serve_3d_min, args.serve_3d_max))
-    server = serving.DiodeServer(max_inflight=16)
+    mixed = args.serve_precision == "mixed"
+    server = serving.DiodeServer(max_inflight=16, mixed=mixed)
     t0 = time.perf_counter()
     res = server.run(reqs)
     wall = time.perf_counter() - t0
@@ -283,7 +285,9 @@ def run_serve(args):
                                    "warm-started Newton; kernel-level continuous batching (one condensation "
                                    "launch per server step over the requests in flight)",
                        "requests": len(reqs), "rate_per_s": args.serve_rate, "seed": 2024,
-                       "max_inflight": server.max_inflight},
+                       "max_inflight": server.max_inflight,
+                       "precision": ("mixed: FP32 Jacobian, FP64 residuals and trace solve (FP64 for 2D "
+                                     "degree 3 and 3D degree 2, which have no mixed kernel)") if mixed else "fp64"},
             "server_steps": server.steps, "peak_batch": server.peak_batch,
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"],
             "solves_per_s": st["solves_per_s"], "cells_per_s": st["cells_per_s"],
@@ -293,13 +297,14 @@ def run_serve(args):
 
 def serve_quick(n=10, rate=4.0, seed=7):
     """A short seeded Poisson stream of small diode solves through the
-    serving layer (2D 32^2..96^2 at degree 1-2, 3D 8^3..12^3 at degree 1):
-    p50 / p99 latency and solves/s, for the default bench line."""
+    serving layer (2D 32^2..96^2 at degree 1-2, 3D 8^3..12^3 at degree 1,
+    mixed-precision condensation): p50 / p99 latency and solves/s, for the
+    default bench line."""
     from ddhdg_b200 import serving
 
-    serving.solve_one(serving.Request(-1, 2, 32, 1, 0.1, 0.0))  # warm the kernels
+    serving.solve_one(serving.Request(-1, 2, 32, 1, 0.1, 0.0), mixed=True)  # warm the kernels
     reqs = serving.poisson_requests(n, rate, seed=seed, sizes_2d=(32, 96), sizes_3d=(8, 12))
-    server = serving.DiodeServer(max_inflight=16)
+    server = serving.DiodeServer(max_inflight=16, mixed=True)
     t0 = time.perf_counter()
     res = server.run(reqs)
     wall = time.perf_counter() - t0
@@ -309,7 +314,7 @@ def serve_quick(n=10, rate=4.0, seed=7):
             "peak_inflight": server.peak_inflight, "peak_batch": server.peak_batch,
             "server_steps": server.steps, "wall_s": wall,
             "workload": "Poisson stream of 2D 32^2..96^2 (k 1-2) and 3D 8^3..12^3 (k 1) diode solves, "
-                        "bias U[0, 0.8] V (full-size stream: bench.py --serve)"}
+                        "bias U[0, 0.8] V, mixed-precision condensation (full-size stream: bench.py --serve)"}
 
 
 def run_bias_sweep(args):
@@ -621,6 +626,8 @@ def main():
                     help="serve a seeded Poisson stream of diode solves and report p50/p99 latency")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=4.0, help="arrivals per second")
+    ap.add_argument("--serve-precision", choices=("mixed", "fp64"), default="mixed",
+                    help="condensation precision of the served solves")
     ap.add_argument("--serve-3d-min", type=int, default=16)
     ap.add_argument("--serve-3d-max", type=int, default=32,
                     help="largest 3D mesh of the stream (the nested-dissection fronts grow as m^4.1 in 3D)")
@@ -810,7 +817,35 @@ def main():
                  "kernel": "condense3_kernel<2,2,float>",
                  "precision": "FP32 Jacobian (local operators, Gauss-Jordan, Y, Schur operands; "
                               "FP64 accumulation of the products), FP64 residuals, FP64 outputs"}
-        del gm
+
+        # the same mixed-precision device through the batched launch (one
+        # persistent launch per stage, graph replay, tiles autotuned)
+        from ddhdg_b200.batch import CondenseBatch
+
+        bm = CondenseBatch([gm])
+        bm.update_trace[0].copy_(dtrace)
+        bm.autotune(reps=2)
+        for _ in range(max(args.warmup, 3)):
+            bm.condense()
+            bm.reconstruct()
+        torch.cuda.synchronize()
+        evb = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps)]
+        replicas.barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            evb[3 * i].record(bm.stream)
+            bm.condense()
+            evb[3 * i + 1].record(bm.stream)
+            bm.reconstruct()
+            evb[3 * i + 2].record(bm.stream)
+        torch.cuda.synchronize()
+        cb = float(np.mean([evb[3 * i].elapsed_time(evb[3 * i + 1]) for i in range(args.steps)]))
+        rb = float(np.mean([evb[3 * i + 1].elapsed_time(evb[3 * i + 2]) for i in range(args.steps)]))
+        cb = replicas.max_over_ranks(cb, dev)
+        mixed["batched"] = {"condense_ms": cb, "reconstruct_ms": rb, "cells_per_s": replicas.job_throughput(nc, cb + rb),
+                            "shape": bm.shape(), "kernel": "batch_condense_kernel<2> (mixed job)"}
+        bm.close()
+        del bm, gm
         torch.cuda.empty_cache()
 
     # ---- the plain FP64 GPU path (the reference's per-cell algorithm as
@@ -893,6 +928,10 @@ def main():
         target["condense_ms"]["mixed"] = mixed["condense_ms"]
         target["condense_speedup_vs_plain"]["mixed"] = pc / mixed["condense_ms"]
         target["newton_step_ms"]["mixed"] = mixed["condense_ms"] + solve_ms + mixed["reconstruct_ms"]
+        mb = mixed["batched"]
+        target["condense_ms"]["batched_mixed"] = mb["condense_ms"]
+        target["condense_speedup_vs_plain"]["batched_mixed"] = pc / mb["condense_ms"]
+        target["newton_step_ms"]["batched_mixed"] = mb["condense_ms"] + solve_ms + mb["reconstruct_ms"]
     base = target["newton_step_ms"]["plain_fp64"]
     target["newton_step_speedup_vs_plain"] = {k: base / v for k, v in target["newton_step_ms"].items()
                                               if k != "plain_fp64"}

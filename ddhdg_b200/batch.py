@@ -20,7 +20,8 @@ from . import _lib
 
 class CondenseBatch:
     """One launch per Newton step over the contexts of `solvers`
-    (``NPSolver`` objects of one dimension, FP64).  The outputs of solver i
+    (``NPSolver`` objects of one dimension, FP64 or mixed precision, each
+    condensed in its own precision).  The outputs of solver i
     are ``tt[i]``, ``rhs[i]``, ``dflag[i]``, ``dval[i]`` (shaped like
     ``NPSolver.assemble_condense``); the reconstruction reads
     ``update_trace[i]`` ([nfaces * 3 * nf]) and writes ``update_cell[i]``.

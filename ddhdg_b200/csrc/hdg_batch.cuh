@@ -9,11 +9,12 @@
 // counter, loads that device's launch parameters into shared memory and runs
 // the per-degree body on the tile's cells (the unit-cell constant tables of
 // every degree travel in the constant bank): four warps on four cells at a time
-// for the warp-per-cell degrees (condense3_cells), the whole CTA on one cell
-// at a time otherwise (condense2_cells).  Tiles are ordered heaviest first;
-// their sizes per degree and the CTAs per SM come from the host's autotuner.
-// Every device's results are bitwise those of its own ddhdg_assemble_condense
-// (same tables, same parameters, same arithmetic).
+// for the warp-per-cell degrees (condense3_cells, FP64 or with the FP32
+// Jacobian of a mixed-precision device), the whole CTA on one cell at a time
+// otherwise (condense2_cells).  Tiles are ordered heaviest first; their sizes
+// per degree and the CTAs per SM come from the host's autotuner.  Every
+// device's results are bitwise those of its own ddhdg_assemble_condense (same
+// tables, same parameters, same arithmetic).
 #pragma once
 
 #include <cstdint>
@@ -36,7 +37,7 @@ namespace ddhdg
     const double *dtrace; // reconstruction: trace update [nfaces][3][nf]
     double       *dcell;  // reconstruction: cell update [ncells][Nc_all]
     int           k;
-    int           pad;
+    int           mixed;  // 1: FP32 Jacobian (condense3_cells<..., float>)
   };
 
   struct BatchTile
@@ -88,7 +89,9 @@ namespace ddhdg
       return C.t3;
   }
 
-  template <int DIM, int K>
+  // JT: the Jacobian type of the warp-per-cell body (the CTA-per-cell
+  // degrees are FP64 only)
+  template <int DIM, int K, typename JT>
   __device__ __forceinline__ void
   batch_condense_tile(const KParams &P, const BatchTabs<DIM> &C, const BatchTile &t, double *smem,
                       int (*piv)[32])
@@ -98,17 +101,31 @@ namespace ddhdg
     else if constexpr (batch_warp<DIM, K>)
       {
         const int    warp = threadIdx.x >> 5;
-        const Ws3Off wo   = ws3_layout(DIM, Dims<DIM, K>::nb, Dims<DIM, K>::nf, P.ncomp, P.ncol, 8);
-        condense3_cells<DIM, K, double>(P, batch_tab<K>(C), smem + warp * wo.total, piv[warp],
-                                        t.begin + warp, t.end, BatchWarp);
+        const Ws3Off wo   = ws3_layout(DIM, Dims<DIM, K>::nb, Dims<DIM, K>::nf, P.ncomp, P.ncol, (int)sizeof(JT));
+        condense3_cells<DIM, K, JT>(P, batch_tab<K>(C), smem + warp * wo.total, piv[warp], t.begin + warp,
+                                    t.end, BatchWarp);
       }
-    else
+    else if constexpr (sizeof(JT) == 8)
       condense2_cells<DIM, K>(P, smem, blockIdx.x, t.begin, t.end, 1);
   }
 
+  // The precisions a batch holds: FP64 devices only, mixed-precision
+  // warp-per-cell devices only, or both.  Each class is its own
+  // instantiation, so that a batch carries only the bodies it runs: the
+  // mixed-only kernel is built for four CTAs per SM (128 registers), the
+  // occupancy of the single-device mixed kernel; the others for two (the
+  // FP64 bodies take 255 registers, and the mixed bodies beside them add
+  // spills).
+  enum BatchPrec : int
+  {
+    BatchFP64  = 0,
+    BatchMixed = 1,
+    BatchBoth  = 2
+  };
+
   // counter: tiles handed out so far (zero at launch)
-  template <int DIM>
-  __global__ void __launch_bounds__(BatchTPB, 2)
+  template <int DIM, int PREC>
+  __global__ void __launch_bounds__(BatchTPB, PREC == BatchMixed ? 4 : 2)
   batch_condense_kernel(const BatchJob *__restrict__ jobs, const BatchTile *__restrict__ tiles,
                         int ntiles, int *counter, const __grid_constant__ BatchTabs<DIM> C)
   {
@@ -128,14 +145,26 @@ namespace ddhdg
         const BatchTile t = tiles[ti];
         batch_load_params(Ps, jobs[t.job].P);
         if (threadIdx.x == 0)
-          s_k = jobs[t.job].k;
+          s_k = jobs[t.job].k + (jobs[t.job].mixed ? 4 : 0);
         __syncthreads();
-        switch (s_k)
+        const int sk = s_k;
+        if constexpr (PREC != BatchMixed)
           {
-            case 1: batch_condense_tile<DIM, 1>(Ps, C, t, smem, piv); break;
-            case 2: batch_condense_tile<DIM, 2>(Ps, C, t, smem, piv); break;
-            case 3: batch_condense_tile<DIM, 3>(Ps, C, t, smem, piv); break;
-            default: break;
+            if (sk == 1)
+              batch_condense_tile<DIM, 1, double>(Ps, C, t, smem, piv);
+            else if (sk == 2)
+              batch_condense_tile<DIM, 2, double>(Ps, C, t, smem, piv);
+            else if (sk == 3)
+              batch_condense_tile<DIM, 3, double>(Ps, C, t, smem, piv);
+          }
+        if constexpr (PREC != BatchFP64)
+          {
+            if (sk == 5)
+              batch_condense_tile<DIM, 1, float>(Ps, C, t, smem, piv);
+            else if (sk == 6)
+              batch_condense_tile<DIM, 2, float>(Ps, C, t, smem, piv);
+            else if (sk == 7)
+              batch_condense_tile<DIM, 3, float>(Ps, C, t, smem, piv);
           }
       }
   }

@@ -1314,6 +1314,52 @@ ddhdg_solve_condensed(ddhdg_ctx *c, const double *tt, const double *rhs, const i
 }
 
 int
+ddhdg_trace_solver_bytes(int dim, const int *n, int degree, int ncomp, int64_t *bytes)
+{
+  if (!n || !bytes)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  if (dim < 1 || dim > 3 || degree < 1 || degree > 3 || ncomp < 1 || ncomp > 3)
+    return fail(DDHDG_BAD_ARG, "dim 1-3, degree 1-3 and 1-3 components");
+  NDSolver::Mesh M;
+  M.dim    = dim;
+  M.ncells = 1;
+  int nf   = 1;
+  for (int a = 0; a < dim; ++a)
+    {
+      if (n[a] < 1)
+        return fail(DDHDG_BAD_ARG, "bad mesh");
+      M.n[a] = n[a];
+      M.ncells *= n[a];
+      if (a > 0)
+        nf *= degree + 1;
+    }
+  // the faces in the layout of ddhdg_ctx_create: direction by direction
+  int64_t off = 0;
+  for (int a = 0; a < dim; ++a)
+    {
+      M.face_off[a] = off;
+      int64_t cnt   = 1;
+      for (int b = 0; b < 3; ++b)
+        {
+          const int e       = (b < dim) ? (n[b] + (b == a ? 1 : 0)) : 1;
+          M.face_ext[a][b] = e;
+          cnt *= e;
+        }
+      off += cnt;
+    }
+  M.nfaces = off;
+  M.F      = 2 * dim;
+  M.nd     = ncomp * nf;
+  NDSolver    nd;
+  std::string err;
+  const int   r = nd.plan(M, err);
+  if (r)
+    return fail(r, err);
+  *bytes = nd.planned_device_bytes();
+  return DDHDG_OK;
+}
+
+int
 ddhdg_set_solver_graphs(ddhdg_ctx *c, int enable)
 {
   if (!c)
@@ -2180,6 +2226,7 @@ struct ddhdg_batch
   int                      ntiles_c = 0, ntiles_r = 0, grid_c = 0, grid_r = 0;
   size_t                   smem_c = 0, smem_r = 0;
   bool                     any_r_global         = false;
+  int                      prec                 = BatchFP64; // the precisions of the jobs
   int                      max_rscratch_per_cta = 0;
   int                      sm_count             = 148;
   cudaStream_t             cap                  = nullptr;
@@ -2210,14 +2257,25 @@ struct ddhdg_batch
 
 namespace
 {
+  template <int D>
   const void *
-  batch_condense_fn(int dim)
+  batch_condense_fn_d(int prec)
+  {
+    switch (prec)
+      {
+        case BatchFP64: return reinterpret_cast<const void *>(batch_condense_kernel<D, BatchFP64>);
+        case BatchMixed: return reinterpret_cast<const void *>(batch_condense_kernel<D, BatchMixed>);
+        default: return reinterpret_cast<const void *>(batch_condense_kernel<D, BatchBoth>);
+      }
+  }
+  const void *
+  batch_condense_fn(int dim, int prec)
   {
     switch (dim)
       {
-        case 1: return reinterpret_cast<const void *>(batch_condense_kernel<1>);
-        case 2: return reinterpret_cast<const void *>(batch_condense_kernel<2>);
-        default: return reinterpret_cast<const void *>(batch_condense_kernel<3>);
+        case 1: return batch_condense_fn_d<1>(prec);
+        case 2: return batch_condense_fn_d<2>(prec);
+        default: return batch_condense_fn_d<3>(prec);
       }
   }
   const void *
@@ -2259,6 +2317,23 @@ namespace
         cudaGraphExecDestroy(b->g_r);
         b->g_r = nullptr;
       }
+    const void *fc = batch_condense_fn(b->dim, b->prec), *fr = batch_reconstruct_fn(b->dim);
+    CK(allow_full_dynamic_smem(fc));
+    CK(allow_full_dynamic_smem(fr));
+    int per_sm_r = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_r, fr, BatchRTPB, b->smem_r));
+    if (per_sm_r < 1)
+      return fail(DDHDG_BAD_ARG, "batched reconstruction kernel does not fit on an SM");
+    // reconstruction tiles: at most rcells_per_tile cells, and small enough
+    // that every CTA of a full grid gets about four
+    int64_t rtile;
+    {
+      int64_t total = 0;
+      for (int64_t nc : b->ncells)
+        total += nc;
+      const int64_t fill = total / ((int64_t)per_sm_r * b->sm_count * 4);
+      rtile              = std::max<int64_t>(16, std::min<int64_t>(b->rcells_per_tile, fill));
+    }
     std::vector<BatchTile> tc, tr;
     for (int j = 0; j < b->n; ++j)
       {
@@ -2267,8 +2342,8 @@ namespace
         const int64_t T  = std::max(1, b->cells_per_tile[k]);
         for (int64_t c0 = 0; c0 < nc; c0 += T)
           tc.push_back(BatchTile{j, 0, c0, std::min(nc, c0 + T)});
-        for (int64_t c0 = 0; c0 < nc; c0 += b->rcells_per_tile)
-          tr.push_back(BatchTile{j, 0, c0, std::min<int64_t>(nc, c0 + b->rcells_per_tile)});
+        for (int64_t c0 = 0; c0 < nc; c0 += rtile)
+          tr.push_back(BatchTile{j, 0, c0, std::min<int64_t>(nc, c0 + rtile)});
       }
     // heaviest tiles first, so that the last tiles handed out are short
     auto cost = [b](const BatchTile &t) { return (double)(t.end - t.begin) * b->cost_per_cell[t.job]; };
@@ -2281,18 +2356,13 @@ namespace
       return r;
     b->ntiles_c     = (int)tc.size();
     b->ntiles_r     = (int)tr.size();
-    const void *fc = batch_condense_fn(b->dim), *fr = batch_reconstruct_fn(b->dim);
-    CK(allow_full_dynamic_smem(fc));
-    CK(allow_full_dynamic_smem(fr));
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fc, BatchTPB, b->smem_c));
     if (per_sm < 1)
       return fail(DDHDG_BAD_ARG, "batched condense kernel does not fit on an SM");
     b->grid_c = std::max(1, std::min(b->ntiles_c, std::min(per_sm, b->ctas_per_sm) * b->sm_count));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fr, BatchRTPB, b->smem_r));
-    if (per_sm < 1)
-      return fail(DDHDG_BAD_ARG, "batched reconstruction kernel does not fit on an SM");
-    b->grid_r = std::max(1, std::min(b->ntiles_r, per_sm * b->sm_count));
+
+    b->grid_r = std::max(1, std::min(b->ntiles_r, per_sm_r * b->sm_count));
     // R blocks outside shared memory (3D degree 2): one slice per CTA
     if (b->any_r_global)
       {
@@ -2308,6 +2378,21 @@ namespace
     return DDHDG_OK;
   }
 
+  template <int D>
+  void
+  batch_launch_condense_d(ddhdg_batch *b, const BatchJob *jobs, const BatchTile *tiles, cudaStream_t s)
+  {
+    static BatchTabs<D>   C; // filled once; the tables do not depend on the device
+    static std::once_flag once;
+    std::call_once(once, [] { fill_batch_tabs<D>(C); });
+    if (b->prec == BatchFP64)
+      batch_condense_kernel<D, BatchFP64><<<b->grid_c, BatchTPB, b->smem_c, s>>>(jobs, tiles, b->ntiles_c, b->counter.p, C);
+    else if (b->prec == BatchMixed)
+      batch_condense_kernel<D, BatchMixed><<<b->grid_c, BatchTPB, b->smem_c, s>>>(jobs, tiles, b->ntiles_c, b->counter.p, C);
+    else
+      batch_condense_kernel<D, BatchBoth><<<b->grid_c, BatchTPB, b->smem_c, s>>>(jobs, tiles, b->ntiles_c, b->counter.p, C);
+  }
+
   int
   batch_launch_condense(ddhdg_batch *b, cudaStream_t s)
   {
@@ -2316,30 +2401,9 @@ namespace
     const BatchTile *tiles = reinterpret_cast<const BatchTile *>(b->d_tiles_c.p);
     switch (b->dim)
       {
-        case 1:
-          {
-            static BatchTabs<1> C; // filled once; the tables do not depend on the device
-            static std::once_flag once;
-            std::call_once(once, [] { fill_batch_tabs<1>(C); });
-            batch_condense_kernel<1><<<b->grid_c, BatchTPB, b->smem_c, s>>>(jobs, tiles, b->ntiles_c, b->counter.p, C);
-          }
-          break;
-        case 2:
-          {
-            static BatchTabs<2> C;
-            static std::once_flag once;
-            std::call_once(once, [] { fill_batch_tabs<2>(C); });
-            batch_condense_kernel<2><<<b->grid_c, BatchTPB, b->smem_c, s>>>(jobs, tiles, b->ntiles_c, b->counter.p, C);
-          }
-          break;
-        default:
-          {
-            static BatchTabs<3> C;
-            static std::once_flag once;
-            std::call_once(once, [] { fill_batch_tabs<3>(C); });
-            batch_condense_kernel<3><<<b->grid_c, BatchTPB, b->smem_c, s>>>(jobs, tiles, b->ntiles_c, b->counter.p, C);
-          }
-          break;
+        case 1: batch_launch_condense_d<1>(b, jobs, tiles, s); break;
+        case 2: batch_launch_condense_d<2>(b, jobs, tiles, s); break;
+        default: batch_launch_condense_d<3>(b, jobs, tiles, s); break;
       }
     CK(cudaGetLastError());
     return DDHDG_OK;
@@ -2451,9 +2515,6 @@ ddhdg_batch_create(const ddhdg_batch_item *items, int n, int thermo, ddhdg_batch
         return fail(DDHDG_BAD_ARG, "batch item " + std::to_string(j) + ": null argument");
       if (c->dim != b->dim)
         return fail(DDHDG_BAD_ARG, "batch items must share one dimension");
-      if (c->desc.precision != 0)
-        return fail(DDHDG_BAD_ARG, "the batched launch is FP64 (item " + std::to_string(j) +
-                                     " has a mixed-precision context)");
       Mode &m = c->mode[thermo];
       if (!m.built)
         set_mode_comps(c, thermo); // host bookkeeping only
@@ -2473,6 +2534,11 @@ ddhdg_batch_create(const ddhdg_batch_item *items, int n, int thermo, ddhdg_batch
       J.dtrace        = it.update_trace;
       J.dcell         = it.update_cell;
       J.k             = c->k;
+      J.mixed         = c->desc.precision == 1 ? 1 : 0; // only where 3 nb <= 32 (ctx_create)
+      {
+        const int jp = J.mixed ? BatchMixed : BatchFP64;
+        b->prec      = (j == 0 || b->prec == jp) ? jp : BatchBoth;
+      }
       const int Ns    = m.ncomp * c->nb;
       b->ycache_off.push_back(ytotal);
       ytotal += ((c->ncells * Ns * m.ycols) + 31) & ~(int64_t)31;
@@ -2482,7 +2548,7 @@ ddhdg_batch_create(const ddhdg_batch_item *items, int n, int thermo, ddhdg_batch
                                  (double)m.Nt * m.Nt * Ns);
       if (3 * c->nb <= 32)
         {
-          const Ws3Off w = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, 8);
+          const Ws3Off w = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, J.mixed ? 4 : 8);
           b->smem_c      = std::max(b->smem_c, (size_t)BatchWarp * w.total * sizeof(double));
           J.P.wpb        = 1;
           J.P.stage      = 0;

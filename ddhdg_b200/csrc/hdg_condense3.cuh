@@ -239,9 +239,7 @@ namespace ddhdg
     const double *TLc    = tb + P.to.TLc;
     const double *TLg    = tb + P.to.TLg;
     const double *TLf    = tb + P.to.TLf;
-    const double *RTk    = tb + P.to.RTk;
     const double *RTr    = tb + P.to.RTr;
-    const double *RQk    = tb + P.to.RQk;
     const double *RQr    = tb + P.to.RQr;
     const double *PW_c   = tb + P.to.PW_c;
     const double *PW_f   = tb + P.to.PW_f;

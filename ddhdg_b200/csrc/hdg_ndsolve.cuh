@@ -21,15 +21,17 @@
 //                           Schur update); above the leaves, while the front
 //                           fits, it is also assembled in shared memory
 //   37..72                  a CTA per front for the LU and W, the Schur update
-//                           as a batched GEMM
+//                           as one tensor-path GEMM launch for the batch
 //   up to 383               own LU, a CTA per front (all fronts at once), then
-//                           batched triangular solves and GEMMs
-//   >= 384 (few fronts)     cuSOLVER LU per front on side streams, triangular
-//                           solves and GEMM per front
-// By default W and the Schur updates of these fronts use cuBLAS (batched or
-// per front); DDHDG_ND_OWN_PRODUCTS=1 switches them to the tensor-path
-// kernels of hdg_ndblas.cuh (measured slower on the 256 x 256 degree-2
-// diode: 100 against 88 ms per solve).
+//                           batched cuBLAS triangular solves and the GEMM launch
+//   >= 384 (few fronts)     cuSOLVER LU and cuBLAS triangular solves per front
+//                           on side streams, then the GEMM launch
+// Above the smallest fronts, the Schur updates F_KK -= F_KE W and the
+// triangular solves for W are cuBLAS calls by default.  Their tensor-path
+// counterparts (hdg_ndblas.cuh: nd_gemm_kernel for all fronts of a batch in
+// one launch, DDHDG_ND_OWN_GEMM=1; 32-row block substitution with inverted
+// diagonal blocks, DDHDG_ND_OWN_TRSM=1) give the same solution to round-off
+// and measured slower at 1.18M dofs.
 // The numeric sequence is captured in a CUDA graph on the second call with
 // the same buffers and replayed afterwards.  Before the factorisation the
 // rows are equilibrated: row g is scaled by 1 / max |row g| over the cells
@@ -1059,6 +1061,46 @@ namespace ddhdg
 
     int64_t front_bytes() const { return front_total_ * (int64_t)sizeof(double); }
 
+    // Device bytes that build() allocates for the planned mesh: fronts,
+    // pivots, inverted diagonal blocks, the maps and the scaling vectors,
+    // each allocation rounded up to the allocator's 2 MiB granularity, plus
+    // a bound of 64 nE doubles per side stream for the LU workspace of the
+    // largest front (the library reports its size only once a handle
+    // exists).  The caller's plan() must have succeeded.
+    int64_t
+    planned_device_bytes() const
+    {
+      const int64_t g = (int64_t)2 << 20;
+      int64_t       b = 0;
+      auto          add = [&](int64_t bytes) { b += (std::max<int64_t>(bytes, 16) + g - 1) / g * g; };
+      add(front_total_ * 8);
+      add(std::max<int64_t>(piv_total_, 1) * 4);
+      add(std::max<int64_t>(piv_total_, 1) * 4);
+      add(((int64_t)nodes_.size() + 1) * 4);
+      int64_t tinv = 1, big_nE = 1;
+      for (const auto &bt : batches_)
+        {
+          if (bt.nE > 0 && !bt.small && !bt.fused && !bt.mid)
+            tinv = std::max<int64_t>(tinv, (int64_t)bt.nodes.size() * ((bt.nE + NDTB - 1) / NDTB) * 2 * NDTB * NDTB);
+          if (bt.big)
+            big_nE = std::max<int64_t>(big_nE, bt.nE);
+        }
+      add(tinv * 8);
+      add((int64_t)fdofs_h_.size() * 4);
+      add((int64_t)emap_h_.size() * 4);
+      add((int64_t)leaf_off_h_.size() * 8);
+      add((int64_t)pmask_h_.size());
+      add((int64_t)cell_faces_.size() * 8);
+      add((int64_t)asm_h_.size() * (int64_t)sizeof(NDAsm));
+      add((int64_t)sol_h_.size() * (int64_t)sizeof(NDSol));
+      add((int64_t)ptr_h_.size() * 8);
+      const int64_t ndofs = M_.nfaces * (int64_t)M_.nd;
+      add(ndofs * 8);
+      add(ndofs * 8);
+      add((int64_t)NSide * 64 * big_nE * 8);
+      return b;
+    }
+
     // the plan's batches: {height, eliminated dofs, kept dofs, fronts, kind}
     // with kind 0 fused, 1 small, 2 mid, 3 own LU + batched products, 4 big
     std::vector<std::vector<int>>
@@ -1097,9 +1139,10 @@ namespace ddhdg
       std::lock_guard<std::mutex> lock(plan_cache_mutex());
       auto &c = plan_cache();
       c.insert(c.begin(), std::move(e));
-      // at most 8 plans, and no more than 4 GB of host copies
+      // at most 32 plans (two modes of 16 requests in flight), and no more
+      // than 4 GB of host copies
       size_t bytes = 0, keep = 0;
-      for (; keep < c.size() && keep < 8; ++keep)
+      for (; keep < c.size() && keep < 32; ++keep)
         {
           bytes += c[keep]->bytes();
           if (bytes > ((size_t)4 << 30) && keep > 0)
@@ -1317,8 +1360,10 @@ namespace ddhdg
             tinv = std::max<int64_t>(tinv, (int64_t)b.nodes.size() * ((b.nE + NDTB - 1) / NDTB) * 2 * NDTB * NDTB);
         if ((r = dmalloc(d_tinv_, tinv * sizeof(double), err)))
           return r;
-        const char *e = getenv("DDHDG_ND_OWN_PRODUCTS");
-        own_blas_     = e && e[0] == '1';
+        const char *e = getenv("DDHDG_ND_OWN_TRSM");
+        own_trsm_     = e && e[0] == '1';
+        const char *g = getenv("DDHDG_ND_OWN_GEMM");
+        own_gemm_     = g && g[0] == '1';
       }
       if ((r = upload(d_fdofs_, fdofs_h_, err)) || (r = upload(d_emap_, emap_h_, err)) ||
           (r = upload(d_leaf_off_, leaf_off_h_, err)) || (r = upload(d_pmask_, pmask_h_, err)) ||
@@ -1672,14 +1717,16 @@ namespace ddhdg
           const dim3 g2(1, (b.nK + 1 + NDPermCols - 1) / NDPermCols);
           nd_rowperm_kernel<<<g2, 256, b.nE * sizeof(double), ss>>>(b.nE, nF, d_sol_ + b.sol_off + q,
                                                                     pm, d_fronts_);
-          if (own_blas_)
-            continue; // W and the Schur update for all fronts at once, below
+          if (own_trsm_)
+            continue; // W for all fronts at once, below
           double *B = Fq + (int64_t)b.nE * nF;
           if (cublasDtrsm(side_blas_[k], CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
                           CUBLAS_DIAG_UNIT, b.nE, b.nK + 1, &one, Fq, nF, B, nF) != CUBLAS_STATUS_SUCCESS ||
               cublasDtrsm(side_blas_[k], CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
                           CUBLAS_DIAG_NON_UNIT, b.nE, b.nK + 1, &one, Fq, nF, B, nF) != CUBLAS_STATUS_SUCCESS)
             return bad(err, "cublasDtrsm failed", DDHDG_SOLVER_ERROR);
+          if (own_gemm_)
+            continue; // the Schur updates of all fronts at once, below
           if (b.nK > 0 &&
               cublasDgemm(side_blas_[k], CUBLAS_OP_N, CUBLAS_OP_N, b.nK, b.nK + 1, b.nE, &mone, Fq + b.nE,
                           nF, B, nF, &one, B + b.nE, nF) != CUBLAS_STATUS_SUCCESS)
@@ -1689,15 +1736,12 @@ namespace ddhdg
         if (cudaEventRecord(ev_join_[k], side_[k]) != cudaSuccess ||
             cudaStreamWaitEvent(s, ev_join_[k], 0) != cudaSuccess)
           return bad(err, "stream join failed", DDHDG_CUDA_ERROR);
-      if (own_blas_)
-        {
-          double **pEE = d_ptr_ + b.ptr_off, **pEK = pEE + nb, **pKE = pEK + nb, **pKK = pKE + nb;
-          int      r;
-          if ((r = solve_w(b, pEE, pEK, s, err)))
-            return r;
-          if (b.nK > 0 && (r = schur_update(b, pKE, pEK, pKK, s, err)))
-            return r;
-        }
+      double **pEE = d_ptr_ + b.ptr_off, **pEK = pEE + nb, **pKE = pEK + nb, **pKK = pKE + nb;
+      int      r;
+      if (own_trsm_ && (r = solve_w(b, pEE, pEK, s, err)))
+        return r;
+      if ((own_trsm_ || own_gemm_) && b.nK > 0 && (r = schur_update(b, pKE, pEK, pKK, s, err)))
+        return r;
       return DDHDG_OK;
     }
 
@@ -1712,7 +1756,7 @@ namespace ddhdg
       // 32 right-hand sides: worth it while there are enough of them (not
       // for the root's single column, nor for the largest 3D fronts)
       const int ntiles = (b.nK + 1 + NDTB - 1) / NDTB;
-      if (own_blas_ && (int64_t)ntiles * nb >= 64 && b.nE <= 1152)
+      if (own_trsm_ && (int64_t)ntiles * nb >= 64 && b.nE <= 1152)
         {
           const int nblk = (b.nE + NDTB - 1) / NDTB;
           nd_trinv_kernel<<<dim3(nblk, nb), 64, 0, s>>>(b.nE, nF, pEE, d_tinv_);
@@ -1736,7 +1780,7 @@ namespace ddhdg
     {
       const int nF = b.nE + b.nK;
       const int nb = (int)b.nodes.size();
-      if (own_blas_)
+      if (own_gemm_ || own_trsm_)
         {
           const int tiles = ((b.nK + NDGM - 1) / NDGM) * ((b.nK + 1 + NDGN - 1) / NDGN);
           nd_gemm_kernel<<<dim3(tiles, nb), 128, 0, s>>>(b.nK, b.nK + 1, b.nE, nF, pKE, pEK, pKK);
@@ -2024,7 +2068,8 @@ namespace ddhdg
     std::vector<void *> allocs_;
     double             *d_fronts_ = nullptr, *d_dscale_ = nullptr, *d_work_ = nullptr;
     double             *d_tinv_   = nullptr; // inverted diagonal blocks of the triangular solves
-    bool                own_blas_ = true;    // tensor-path kernels for W and the Schur updates
+    bool                own_trsm_ = false;   // tensor-path triangular solves for W
+    bool                own_gemm_ = false;   // tensor-path Schur updates
     double            **d_ptr_    = nullptr;
     int                *d_piv_ = nullptr, *d_perm_ = nullptr, *d_info_ = nullptr;
     int32_t            *d_fdofs_ = nullptr, *d_emap_ = nullptr;

@@ -373,7 +373,17 @@ namespace ddhdg
             const int bi = P.comps[i / ((DIM + 1) * nb)], si = (i / nb) % (DIM + 1), ai = i % nb;
             const int bj = P.comps[j / ((DIM + 1) * nb)], sj = (j / nb) % (DIM + 1), aj = j % nb;
             double    s  = 0.;
-            for (int q = 0; q < nqc; ++q)
+            // the (test, trial) kinds with a volume term at all (the others
+            // are structural zeros of the reference's loops)
+            bool vol;
+            if (bi == 0)
+              vol = (si < DIM) ? (bj == 0 && (sj == DIM || sj == si))
+                               : ((bj == 0 && sj < DIM) ||
+                                  (sj == DIM && (phi_mode ? bj == 0 : bj != 0)));
+            else
+              vol = (si < DIM) ? (bj == bi && (sj == DIM || sj == si))
+                               : (bj == bi || (bj == 0 && sj < DIM) || (sj == DIM && bj != 0));
+            for (int q = 0; vol && q < nqc; ++q)
               {
                 const double  w  = w_c[q];
                 const double  pi = phi_c[q * nb + ai], pj = phi_c[q * nb + aj];
@@ -799,12 +809,13 @@ namespace ddhdg
                   A[p * ldA + jj] = t;
                 }
             __syncthreads();
+            // rank-1 update: lanes over columns, warps over rows
             const double inv = 1. / A[k * ldA + k];
-            for (int jj = k + 1 + tid; jj < ncols; jj += T)
+            for (int jj = k + 1 + (tid & 31); jj < ncols; jj += 32)
               {
                 const double u = A[k * ldA + jj] * inv;
                 if (u != 0.)
-                  for (int ii = k + 1; ii < Nc; ++ii)
+                  for (int ii = k + 1 + (tid >> 5); ii < Nc; ii += T / 32)
                     A[ii * ldA + jj] -= A[ii * ldA + k] * u;
               }
             __syncthreads();
@@ -816,16 +827,19 @@ namespace ddhdg
             __syncthreads();
             continue;
           }
-        // back substitution U X = Y: a thread per right-hand-side column,
-        // reading only U (no barrier between the steps)
-        for (int jj = Nc + tid; jj < ncols; jj += T)
+        // back substitution U X = Y: a warp per right-hand-side column,
+        // lanes over the rows (no barrier between the steps)
+        for (int jj = Nc + (tid >> 5); jj < ncols; jj += T / 32)
           for (int kk = Nc - 1; kk >= 0; --kk)
             {
               const double x = A[kk * ldA + jj] / A[kk * ldA + kk];
-              A[kk * ldA + jj] = x;
+              __syncwarp();
+              if ((tid & 31) == 0)
+                A[kk * ldA + jj] = x;
               if (x != 0.)
-                for (int ii = 0; ii < kk; ++ii)
+                for (int ii = tid & 31; ii < kk; ii += 32)
                   A[ii * ldA + jj] -= A[ii * ldA + kk] * x;
+              __syncwarp();
             }
         __syncthreads();
 

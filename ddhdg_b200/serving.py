@@ -58,12 +58,35 @@ class Result:
         return self.finish - self.arrival
 
 
+def trace_solver_bytes(dim: int, m: int, k: int, ncomp: int) -> int:
+    """Device bytes of the nested-dissection trace solver of an m^dim mesh
+    at degree k with `ncomp` enabled components, from the solver's own plan
+    (``ddhdg_trace_solver_bytes``: host only; the plan is cached and reused
+    by the solver that the request builds)."""
+    import ctypes
+
+    from . import _lib
+
+    L = _lib.load()
+    n = (ctypes.c_int * 3)(m, m, m)
+    out = ctypes.c_int64()
+    _lib.check(L.ddhdg_trace_solver_bytes(int(dim), n, int(k), int(ncomp), ctypes.byref(out)),
+               "trace_solver_bytes")
+    return int(out.value)
+
+
+# Device bytes of one request beyond its arrays: the library handles of the
+# trace solver's side streams (two modes), its CUDA graphs and the context's
+# streams and events
+REQUEST_OVERHEAD = 1 << 30
+
+
 def memory_estimate(dim: int, m: int, k: int) -> int:
-    """Device bytes of one solve: states, condensed blocks, the Y cache and
-    the fronts of the nested-dissection trace solve (the fronts dominate;
-    per cell about 320 nd^2 log2(m) bytes in 2D, and about m^4.1 in all in
-    3D, nd the trace dofs per face, fitted to the solver's own plans and
-    rounded up)."""
+    """Device bytes of one solve: the trace solvers of both phases (the
+    biased system and the V-only equilibrium system, which stays allocated
+    for the rest of the solve) from their plans, the global trace sparsity,
+    the per-cell states, condensed blocks and Y cache of both phases, and the
+    per-request overhead; the array terms 10 % over."""
     nb = (k + 1) ** dim
     nf = (k + 1) ** (dim - 1)
     cells = m ** dim
@@ -71,19 +94,15 @@ def memory_estimate(dim: int, m: int, k: int) -> int:
     Ns = 3 * nb
     nd = 3 * nf
     per_cell = 8 * (3 * (dim + 1) * nb * 3 + Nt * Nt + 3 * Nt + Ns * (1 + Nt))
-    # the fronts of the full system, plus those of the equilibrium (V only,
-    # (1/3)^2 of them), which stay allocated for the rest of the solve
-    if dim == 1:
-        fronts = 64 * nd * nd * cells
-    elif dim == 2:
-        fronts = 320 * nd * nd * max(math.log2(m), 1.0) * cells
-    else:
-        # the solver's plans at degree 1: 5.5 GB at 16^3, 29.9 GB at 24^3,
-        # 94.9 GB at 32^3 (about m^4.1), 10 % over
-        fronts = 1.1 * 5.5e9 * (m / 16.0) ** 4.1 * (nd / 12.0) ** 2
-    fronts *= 1.0 + 1.0 / 9.0
-    # two sets of per-cell buffers (equilibrium and biased phases)
-    return int(2 * per_cell * cells + fronts + (64 << 20))
+    # the batched launch keeps its own Y cache of the request's cells
+    batch_y = 8 * Ns * (1 + Nt)
+    fronts = trace_solver_bytes(dim, m, k, 3) + trace_solver_bytes(dim, m, k, 1)
+    # the global trace sparsity of both modes (values, column indices and
+    # the permutation maps: about 20 bytes per nonzero; a face couples to
+    # the 4 dim - 1 faces of its two cells)
+    faces = dim * (m + 1) * m ** (dim - 1)
+    csr = 20 * faces * nd * nd * (4 * dim - 1) * (1.0 + 1.0 / 9.0)
+    return int(1.1 * ((2 * per_cell + batch_y) * cells + fronts + csr)) + REQUEST_OVERHEAD
 
 
 def poisson_requests(n: int, rate: float, seed: int, sizes_2d=(32, 256), sizes_3d=(8, 16),
@@ -107,12 +126,19 @@ def poisson_requests(n: int, rate: float, seed: int, sizes_2d=(32, 256), sizes_3
     return out
 
 
-def solve_one(req: Request, device="cuda:0", keep_state=False, tol=1e-10, max_it=50):
+def request_precision(req: Request, mixed: bool) -> int:
+    """The context precision of a request: 1 (FP32 Jacobian, FP64 residuals)
+    when `mixed` and its degree has a mixed-precision kernel
+    (3 (k+1)^dim <= 32), else 0 (FP64)."""
+    return 1 if mixed and 3 * (req.k + 1) ** req.dim <= 32 else 0
+
+
+def solve_one(req: Request, device="cuda:0", keep_state=False, tol=1e-10, max_it=50, mixed=False):
     """One request's solve on the calling thread's current CUDA stream."""
     from . import workloads
     from .solver import NPSolver
 
-    pb, prm, adim = workloads.diode(dim=req.dim, m=req.m, k=req.k)
+    pb, prm, adim = workloads.diode(dim=req.dim, m=req.m, k=req.k, precision=request_precision(req, mixed))
     prm.consistent_drift_jacobian = True
     prm.consistent_recombination_jacobian = True
     g = NPSolver(pb, prm, adim, device=device)
@@ -134,10 +160,14 @@ class ThreadedDiodeServer:
     hbm_reserve: bytes of device memory left free for everything else.
     hbm_limit: treat the device as having at most this many bytes (tests).
     mem_info: callable returning (free, total) device bytes; defaults to
-    cudaMemGetInfo of `device`."""
+    cudaMemGetInfo of `device`.
+    mixed: condense with the FP32 Jacobian and FP64 residuals where the
+    request's degree has that kernel (the Newton loop converges to the FP64
+    solution)."""
 
     def __init__(self, max_inflight=8, hbm_reserve=4 << 30, hbm_limit=None, device="cuda:0",
-                 keep_states=False, mem_info=None):
+                 keep_states=False, mem_info=None, mixed=False):
+        self.mixed = mixed
         self.max_inflight = max_inflight
         self.hbm_reserve = hbm_reserve
         self.hbm_limit = hbm_limit
@@ -198,7 +228,7 @@ class ThreadedDiodeServer:
             try:
                 stream = torch.cuda.Stream(device=self.device)
                 with torch.cuda.stream(stream):
-                    conv, it, cells, state = solve_one(req, self.device, self.keep_states)
+                    conv, it, cells, state = solve_one(req, self.device, self.keep_states, mixed=self.mixed)
                     stream.synchronize()
                 finish = time.perf_counter() - t0
                 res = Result(req.rid, req.arrival, start, finish, it, conv, cells, state)
@@ -279,8 +309,8 @@ class DiodeServer(ThreadedDiodeServer):
     ``ThreadedDiodeServer``."""
 
     def __init__(self, max_inflight=16, hbm_reserve=4 << 30, hbm_limit=None, device="cuda:0",
-                 keep_states=False, mem_info=None, tol=1e-10, max_it=50):
-        super().__init__(max_inflight, hbm_reserve, hbm_limit, device, keep_states, mem_info)
+                 keep_states=False, mem_info=None, tol=1e-10, max_it=50, mixed=False):
+        super().__init__(max_inflight, hbm_reserve, hbm_limit, device, keep_states, mem_info, mixed)
         self.tol = tol
         self.max_it = max_it
         self.steps = 0
@@ -291,7 +321,8 @@ class DiodeServer(ThreadedDiodeServer):
         from .solver import NPSolver
 
         req = a.req
-        pb, prm, adim = workloads.diode(dim=req.dim, m=req.m, k=req.k)
+        pb, prm, adim = workloads.diode(dim=req.dim, m=req.m, k=req.k,
+                                        precision=request_precision(req, self.mixed))
         prm.consistent_drift_jacobian = True
         prm.consistent_recombination_jacobian = True
         g = NPSolver(pb, prm, adim, device=self.device)

@@ -101,11 +101,13 @@ def bias_sweep(solver, problem, biases, absolute_tol=None, relative_tol=None,
 
 
 def batch_diodes(n, seed=3, sizes=(16, 128), degrees=(1, 2, 3), doping=(1e21, 1e24), junction=(0.3, 0.7),
-                 dim=2):
+                 dim=2, mixed=False):
     """Seeded heterogeneous batch of diodes shaped like the batched benchmark
     configuration: mesh cells per side uniform in `sizes`, degree uniform in
     `degrees`, doping (N_D = N_A) log-uniform in `doping`, junction position
-    uniform in `junction` (fraction of the length).  Returns a list of
+    uniform in `junction` (fraction of the length); with `mixed`, the
+    devices whose degree has a mixed-precision kernel (3 (k+1)^dim <= 32)
+    condense with the FP32 Jacobian, the others in FP64.  Returns a list of
     (problem, parameters, adimensionalizer, spec dict)."""
     import numpy as np
 
@@ -116,6 +118,7 @@ def batch_diodes(n, seed=3, sizes=(16, 128), degrees=(1, 2, 3), doping=(1e21, 1e
         k = int(rng.choice(degrees))
         N = float(10 ** rng.uniform(math.log10(doping[0]), math.log10(doping[1])))
         xj = float(rng.uniform(*junction))
-        pb, prm, adim = diode(dim=dim, m=m, k=k, N_D=N, N_A=N, x_j=xj)
-        out.append((pb, prm, adim, dict(m=m, k=k, doping=N, x_j=xj)))
+        prec = 1 if mixed and 3 * (k + 1) ** dim <= 32 else 0
+        pb, prm, adim = diode(dim=dim, m=m, k=k, N_D=N, N_A=N, x_j=xj, precision=prec)
+        out.append((pb, prm, adim, dict(m=m, k=k, doping=N, x_j=xj, precision=prec)))
     return out

@@ -250,6 +250,15 @@ int ddhdg_solve_condensed(ddhdg_ctx *ctx, const double *tt, const double *rhs,
  * that make only a couple of solves per context.  Both give the same bits. */
 int ddhdg_set_solver_graphs(ddhdg_ctx *ctx, int enable);
 
+/* No counterpart in the reference (its solve is UMFPACK or GMRES on the
+ * host).  Device bytes that the trace solver of a structured mesh allocates
+ * (fronts, pivots, maps), from its host-side plan alone: `dim`, cells per
+ * direction n[0..dim-1], `degree` and the enabled components `ncomp` (1-3;
+ * 1 for the thermodynamic-equilibrium system).  No device is touched; the
+ * plan is kept in the process-wide cache, so a solver built later on the same
+ * mesh reuses it.  For memory admission of a serving layer. */
+int ddhdg_trace_solver_bytes(int dim, const int *n, int degree, int ncomp, int64_t *bytes);
+
 /* assemble_system(true, thermo_eq): cell update from the full trace update
  * update_trace [nfaces][3][nf] (include/assembling_methods.template.h:
  * 2122-2160 and 2688-2697).  Uses the reconstruction data kept by the last
@@ -342,7 +351,8 @@ int ddhdg_reference_points(int dim, int degree, double *qref_c, double *qref_f,
  * include/assembling_methods.template.h:67-88); a batch hands out tiles
  * (device, range of its cells) from a work list to the CTAs of one grid.
  * Every device's outputs are bitwise those of its own
- * ddhdg_assemble_condense / ddhdg_reconstruct.  FP64 contexts only.  The
+ * ddhdg_assemble_condense / ddhdg_reconstruct.  FP64 and mixed-precision
+ * contexts may share a batch (each keeps its own precision).  The
  * pointers of an item are fixed for the life of the batch (the launches
  * are replayed from CUDA graphs); the batch keeps its own reconstruction
  * data, so ddhdg_batch_reconstruct follows ddhdg_batch_condense. */

@@ -114,7 +114,7 @@ def test_batch_against_the_oracle():
         assert np.array_equal(batch.dflag[i].cpu().numpy(), o.assemble_condense()[2])
 
 
-def test_batch_rejects_mixed_dimensions_and_precisions():
+def test_batch_rejects_mixed_dimensions():
     from ddhdg_b200._lib import DDHDGError
     from ddhdg_b200.batch import CondenseBatch
 
@@ -122,6 +122,22 @@ def test_batch_rejects_mixed_dimensions_and_precisions():
     b = _solvers([workloads.diode(dim=1, m=8, k=1) + ({},)])
     with pytest.raises(DDHDGError, match="one dimension"):
         CondenseBatch(a + b)
-    c = _solvers([workloads.diode(dim=2, m=4, k=1, precision=1) + ({},)])
-    with pytest.raises(DDHDGError, match="FP64"):
-        CondenseBatch(a + c)
+
+
+@pytest.mark.parametrize("dim,sizes,degrees", [(2, (6, 20), (1, 2, 3)), (3, (2, 4), (1, 2)), (2, (6, 20), (1, 2))])
+def test_mixed_precision_devices_in_a_batch(dim, sizes, degrees):
+    """FP64 and mixed-precision devices in one launch (or mixed ones only,
+    which take the kernel built for four CTAs per SM): each device's outputs
+    are bitwise those of its own context (the mixed ones from the FP32-
+    Jacobian kernel), whatever the tile shape."""
+    from ddhdg_b200.batch import CondenseBatch
+
+    specs = workloads.batch_diodes(8, seed=20 + dim, sizes=sizes, degrees=degrees, dim=dim, mixed=True)
+    precs = {s[3]["precision"] for s in specs}
+    assert precs == ({0, 1} if 3 in degrees or dim == 3 else {1})
+    solvers = _solvers(specs, seed=4)
+    batch = CondenseBatch(solvers)
+    _check_bitwise(batch, solvers)
+    batch.set_shape({1: 4, 2: 8, 3: 1}, 1)
+    _check_bitwise(batch, solvers)
+    batch.close()

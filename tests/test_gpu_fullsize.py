@@ -35,6 +35,28 @@ def _sample_cells(m, n_interior=1024, seed=7):
     return np.sort(np.concatenate([special, rng.choice(rest, size=n_interior, replace=False)]))
 
 
+def _oracle_residuals(o, m, nf, n_pairs=256, seed=11):
+    """The oracle's equations at its current state on a sample of an m x m
+    mesh: the cell-equation residuals (cc_rhs) of the sampled cells, and the
+    trace-equation residuals assembled on faces whose two cells are both in
+    the sample (the sum of the two cells' tt_rhs rows of that face).  Both
+    vanish at a solution of the discrete problem."""
+    rng = np.random.default_rng(seed)
+    ix = np.arange(m * m) % m
+    iy = np.arange(m * m) // m
+    base = rng.choice(np.flatnonzero((ix < m - 1) & (iy < m - 1)), size=n_pairs, replace=False)
+    cells = np.unique(np.concatenate([base, base + 1, base + m]))
+    pos = {int(c): i for i, c in enumerate(cells)}
+    _, _, _, _, c_rhs, t_rhs = o.local_cell_systems(cells=cells)
+    rows = lambda f: slice(f * 3 * nf, (f + 1) * 3 * nf)  # trace rows of local face f, [f][component][node]
+    faces = []
+    for c in base:
+        a = t_rhs[pos[int(c)]]
+        faces.append(a[rows(1)] + t_rhs[pos[int(c) + 1]][rows(0)])  # x face between c and c + 1
+        faces.append(a[rows(3)] + t_rhs[pos[int(c) + m]][rows(2)])  # y face between c and c + m
+    return c_rhs, np.array(faces)
+
+
 def _residual_of(torch, g, x):
     """(A x - b, b) for the assembled system, from the per-cell blocks."""
     sysm = g._system
@@ -94,15 +116,18 @@ def test_full_size_solve_and_newton():
     o = OracleSolver(pb, prm, adim)
     sel = _sample_cells(256)
     assert sel.size >= 1024
-    # the converged fields solve the oracle's equations: its condensed
-    # residual on the sample is 1e8 times below the one at the start state
+    # the converged fields solve the oracle's equations: its cell residuals
+    # and its assembled face residuals on a sample are 1e8 times below the
+    # ones at the start state
     o.cell_state[:], o.trace_state[:] = start
-    _, g_start = o.condense_accurate(cells=sel)
+    c_start, f_start = _oracle_residuals(o, 256, g.nf)
     o.cell_state[:] = g.get_cell_state()
     o.trace_state[:] = g.get_trace_state()
-    _, g_conv = o.condense_accurate(cells=sel)
-    print(f"oracle residual on the sample: start {np.abs(g_start).max():.3e}, converged {np.abs(g_conv).max():.3e}")
-    assert np.abs(g_conv).max() <= 1e-8 * np.abs(g_start).max()
+    c_conv, f_conv = _oracle_residuals(o, 256, g.nf)
+    print(f"oracle residuals on the sample: cells {np.abs(c_start).max():.3e} -> {np.abs(c_conv).max():.3e}, "
+          f"faces {np.abs(f_start).max():.3e} -> {np.abs(f_conv).max():.3e}")
+    assert np.abs(c_conv).max() <= 1e-8 * np.abs(c_start).max()
+    assert np.abs(f_conv).max() <= 1e-8 * np.abs(f_start).max()
     rng = np.random.default_rng(21)
     for perturbed in (False, True):
         cs, ts = g.get_cell_state(), g.get_trace_state()
@@ -160,17 +185,16 @@ def test_full_size_mixed_newton_matches_fp64():
     print(f"256x256 k=2, 0.3 V: FP64 {r64.iterations} iterations, mixed {rm.iterations}; "
           f"final field difference {err:.2e}")
     assert err < 1e-8, err
-    # the mixed result against the oracle's own equations (FP64): its
-    # condensed residual on a sample of cells is 1e8 times below the start's
+    # the mixed result against the oracle's own equations (FP64): its cell
+    # and assembled face residuals on a sample are 1e8 times below the start's
     from oracle.oracle import OracleSolver
-    from tests.test_gpu_fullsize import _sample_cells as sample
 
     o = OracleSolver(pbm, prmm, adimm)
-    sel = sample(256, n_interior=512)
     o.cell_state[:], o.trace_state[:] = start
-    _, g_start = o.condense_accurate(cells=sel)
+    c_start, f_start = _oracle_residuals(o, 256, 3)
     o.cell_state[:], o.trace_state[:] = c32, t32
-    _, g_conv = o.condense_accurate(cells=sel)
-    print(f"oracle residual at the mixed solution: start {np.abs(g_start).max():.3e}, "
-          f"converged {np.abs(g_conv).max():.3e}")
-    assert np.abs(g_conv).max() <= 1e-8 * np.abs(g_start).max()
+    c_conv, f_conv = _oracle_residuals(o, 256, 3)
+    print(f"oracle residuals at the mixed solution: cells {np.abs(c_start).max():.3e} -> "
+          f"{np.abs(c_conv).max():.3e}, faces {np.abs(f_start).max():.3e} -> {np.abs(f_conv).max():.3e}")
+    assert np.abs(c_conv).max() <= 1e-8 * np.abs(c_start).max()
+    assert np.abs(f_conv).max() <= 1e-8 * np.abs(f_start).max()

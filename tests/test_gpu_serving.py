@@ -83,3 +83,76 @@ def test_batched_server_memory_admission():
     assert server.peak_committed <= limit
     total = sum(serving.memory_estimate(r.dim, r.m, r.k) for r in reqs)
     assert server.peak_committed < total
+
+
+@pytest.mark.parametrize("dim,m,k", [(2, 64, 2), (3, 8, 1)])
+def test_memory_estimate_bounds_a_request(dim, m, k):
+    """The device memory a request takes at its peak (sampled from another
+    thread through the whole solve) stays below its admission estimate."""
+    import gc
+    import threading
+    import time
+
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    serving.solve_one(serving.Request(-1, 2, 16, 1, 0.1, 0.0))  # library state outside the request
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    free0, _ = torch.cuda.mem_get_info()
+    peak, stop = [0], [False]
+
+    def poll():
+        while not stop[0]:
+            free, _ = torch.cuda.mem_get_info()
+            peak[0] = max(peak[0], free0 - free)
+            time.sleep(0.005)
+
+    th = threading.Thread(target=poll, daemon=True)
+    th.start()
+    try:
+        res = serving.DiodeServer(max_inflight=2).run([serving.Request(0, dim, m, k, 0.3, 0.0)])
+        torch.cuda.synchronize()
+    finally:
+        stop[0] = True
+        th.join()
+    assert res[0].converged
+    assert 0 < peak[0] <= serving.memory_estimate(dim, m, k)
+
+
+def test_mixed_precision_server():
+    """Mixed-precision condensation in the batched server: each result is
+    the same alone and in the mix (bitwise), and the final fields agree with
+    the FP64 server's to 1e-8 relative."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    reqs = _requests()
+    alone = serving.DiodeServer(max_inflight=1, keep_states=True, mixed=True).run(reqs)
+    server = serving.DiodeServer(max_inflight=8, keep_states=True, mixed=True)
+    mix = server.run(reqs)
+    assert server.peak_batch > 1
+    fp64 = serving.DiodeServer(max_inflight=8, keep_states=True).run(reqs)
+    for r, a, b, c in zip(reqs, alone, mix, fp64):
+        assert a.converged and b.converged and c.converged
+        assert a.iterations == b.iterations
+        for x, y in zip(a.state, b.state):
+            assert np.array_equal(x, y), a.rid
+        # per component block: cells [cell][V, n, p][flux axes, value][node],
+        # trace [face][V, n, p][node]
+        cell_x = a.state[0].reshape(r.m ** r.dim, 3, r.dim + 1, -1)
+        cell_z = c.state[0].reshape(cell_x.shape)
+        trace_x = a.state[1].reshape(-1, 3, (r.k + 1) ** (r.dim - 1))
+        trace_z = c.state[1].reshape(trace_x.shape)
+        # a block's scale is its largest magnitude, floored at 1e-6 of its
+        # component's largest (blocks that vanish physically, such as E_y of
+        # these diodes, hold round-off only)
+        for b_ in range(3):
+            comp = np.max(np.abs(cell_z[:, b_]))
+            for s_ in range(r.dim + 1):
+                z = cell_z[:, b_, s_]
+                scale = max(np.max(np.abs(z)), 1e-6 * comp)
+                assert np.max(np.abs(cell_x[:, b_, s_] - z)) <= 1e-8 * scale, (a.rid, b_, s_)
+            z = trace_z[:, b_]
+            assert np.max(np.abs(trace_x[:, b_] - z)) <= 1e-8 * np.max(np.abs(z)), (a.rid, b_)

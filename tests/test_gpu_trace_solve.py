@@ -114,9 +114,10 @@ def test_solver_graphs_switch_gives_the_same_solution():
 
 def test_tensor_path_products_match_the_library_ones(monkeypatch):
     """W = U^-1 L^-1 [F_EK | r_E] and the Schur updates on the FP64 tensor
-    path (inverted 32 x 32 diagonal blocks, hdg_ndblas.cuh; the switch
-    DDHDG_ND_OWN_PRODUCTS=1 is read when a context builds its solver)
-    against the same solve with cuBLAS's triangular solves and products:
+    path (inverted 32 x 32 diagonal blocks, hdg_ndblas.cuh; the switches
+    DDHDG_ND_OWN_TRSM / DDHDG_ND_OWN_GEMM are read when a context builds
+    its solver) against the same solve with cuBLAS's triangular solves and
+    products:
     the same solution to round-off, on a mesh whose top fronts take the
     per-front LU path."""
     torch, g = _setup(2, 48, 2)
@@ -124,7 +125,8 @@ def test_tensor_path_products_match_the_library_ones(monkeypatch):
     n = g.sizes().n_trace_dofs
     xs = []
     for own in ("1", "0"):
-        monkeypatch.setenv("DDHDG_ND_OWN_PRODUCTS", own)
+        monkeypatch.setenv("DDHDG_ND_OWN_TRSM", own)
+        monkeypatch.setenv("DDHDG_ND_OWN_GEMM", own)
         _, h = _setup(2, 48, 2)  # a fresh context builds its own solver
         x = torch.full((n,), float("nan"), dtype=torch.float64, device=g.device)
         _lib.check(h.L.ddhdg_solve_condensed(h._ctx, tt.data_ptr(), rhs.data_ptr(), fl.data_ptr(),

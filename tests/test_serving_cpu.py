@@ -39,3 +39,13 @@ def test_estimates_grow_with_the_problem():
     e = serving.memory_estimate
     assert e(2, 64, 2) > e(2, 32, 2) > e(2, 32, 1)
     assert e(3, 16, 1) > e(3, 8, 1)
+
+
+def test_trace_solver_bytes_come_from_the_plan():
+    b3 = serving.trace_solver_bytes(2, 32, 2, 3)
+    b1 = serving.trace_solver_bytes(2, 32, 2, 1)
+    assert b3 > b1 > 0
+    assert serving.trace_solver_bytes(2, 64, 2, 3) > b3
+    assert serving.trace_solver_bytes(3, 8, 1, 3) > serving.trace_solver_bytes(3, 6, 1, 3)
+    # the estimate holds both modes' solvers
+    assert serving.memory_estimate(2, 32, 2) > b3 + b1
