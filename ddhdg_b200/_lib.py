@@ -31,7 +31,7 @@ EXPORTS = [
     "ddhdg_set_solver_graphs", "ddhdg_local_cell_system", "ddhdg_assemble_condense_plain",
     "ddhdg_reconstruct_plain", "ddhdg_sample_points", "ddhdg_batch_create", "ddhdg_batch_destroy",
     "ddhdg_batch_condense", "ddhdg_batch_reconstruct", "ddhdg_batch_set_shape", "ddhdg_batch_get_shape",
-    "ddhdg_batch_autotune", "ddhdg_batch_newton_step", "ddhdg_trace_solver_bytes",
+    "ddhdg_batch_autotune", "ddhdg_batch_newton_step", "ddhdg_trace_solver_bytes", "ddhdg_release_solver",
 ]
 
 
@@ -107,6 +107,7 @@ def load(build_if_missing: bool = True):
     L.ddhdg_reconstruct_host.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p]
     L.ddhdg_set_solver_graphs.argtypes = [c_void_p, c_int]
     L.ddhdg_trace_solver_bytes.argtypes = [c_int, P(c_int), c_int, c_int, P(c_int64)]
+    L.ddhdg_release_solver.argtypes = [c_void_p, c_int]
     L.ddhdg_local_cell_system.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int64, c_void_p,
                                           c_int64] + [c_void_p] * 7
     L.ddhdg_assemble_condense_plain.argtypes = L.ddhdg_assemble_condense.argtypes

@@ -585,26 +585,24 @@ namespace
       }
   }
 
-  // chunk size, table staging and placement of the right-hand-side block R
-  // so that one cell's workspace (one CTA of CondenseTPB threads) fits in
-  // the 227 KB of shared memory of a CTA; R moves to global memory only when
-  // nothing else makes it fit
+  // table staging and placement of the right-hand-side block R so that one
+  // cell's workspace (one CTA of CondenseTPB threads) fits in the 227 KB of
+  // shared memory of a CTA; R moves to global memory only when nothing else
+  // makes it fit
   int
-  launch_shape(const ddhdg_ctx *c, const Mode &m, int &chunk, int &stage, bool &r_global,
-               size_t &smem)
+  launch_shape(const ddhdg_ctx *c, const Mode &m, int &stage, bool &r_global, size_t &smem)
   {
     const size_t limit = 220 * 1024;
     const size_t tb    = (((size_t)c->to.total + 1) & ~(size_t)1) * sizeof(double);
     for (int rg = 0; rg < 2; ++rg)
       for (stage = 1; stage >= 0; --stage)
-        for (chunk = 16; chunk >= 1; chunk /= 2)
-          {
-            r_global       = rg != 0;
-            const Ws2Off w = ws2_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, chunk, r_global);
-            smem           = (stage ? tb : 0) + (size_t)w.total * sizeof(double);
-            if (smem <= limit)
-              return DDHDG_OK;
-          }
+        {
+          r_global       = rg != 0;
+          const Ws2Off w = ws2_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, r_global);
+          smem           = (stage ? tb : 0) + (size_t)w.total * sizeof(double);
+          if (smem <= limit)
+            return DDHDG_OK;
+        }
     return fail(DDHDG_BAD_ARG, "the per-cell workspace does not fit in shared memory");
   }
 
@@ -1251,12 +1249,11 @@ condense_range(ddhdg_ctx *c, const double *cell_state, const double *trace_state
     }
   else
     {
-      int  chunk, stage;
+      int  stage;
       bool r_global;
-      if ((r = launch_shape(c, m, chunk, stage, r_global, smem)))
+      if ((r = launch_shape(c, m, stage, r_global, smem)))
         return r;
       P.wpb   = 1;
-      P.chunk = chunk;
       P.stage = stage;
       threads = CondenseTPB;
       units   = c1 - c0;
@@ -1356,6 +1353,16 @@ ddhdg_trace_solver_bytes(int dim, const int *n, int degree, int ncomp, int64_t *
   if (r)
     return fail(r, err);
   *bytes = nd.planned_device_bytes();
+  return DDHDG_OK;
+}
+
+int
+ddhdg_release_solver(ddhdg_ctx *c, int thermo)
+{
+  if (!c)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  CK(cudaDeviceSynchronize()); // no solve of this context may be in flight
+  c->mode[thermo ? 1 : 0].nd.reset();
   return DDHDG_OK;
 }
 
@@ -1876,11 +1883,10 @@ ddhdg_assemble_condense_noalloc(ddhdg_ctx *c, const double *cell_state,
     }
   else
     {
-      int chunk, stage;
-      if ((r = launch_shape(c, m, chunk, stage, r_global, smem)))
+      int stage;
+      if ((r = launch_shape(c, m, stage, r_global, smem)))
         return r;
       P.wpb   = 1;
-      P.chunk = chunk;
       P.stage = stage;
       threads = CondenseTPB;
       units   = c->ncells;
@@ -2221,7 +2227,8 @@ struct ddhdg_batch
   DevBuf<int>              counter; // [0]: condense, [1]: reconstruct
   bool                     degrees[4]        = {false, false, false, false};
   int                      cells_per_tile[4] = {0, 32, 32, 4};
-  int                      ctas_per_sm       = 2;
+  int                      ctas_per_sm       = 4; // at most; the kernel's occupancy limit applies
+  int                      occ_c             = 0; // CTAs per SM the condense kernel allows
   int                      rcells_per_tile   = 256;
   int                      ntiles_c = 0, ntiles_r = 0, grid_c = 0, grid_r = 0;
   size_t                   smem_c = 0, smem_r = 0;
@@ -2360,6 +2367,7 @@ namespace
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fc, BatchTPB, b->smem_c));
     if (per_sm < 1)
       return fail(DDHDG_BAD_ARG, "batched condense kernel does not fit on an SM");
+    b->occ_c  = per_sm;
     b->grid_c = std::max(1, std::min(b->ntiles_c, std::min(per_sm, b->ctas_per_sm) * b->sm_count));
 
     b->grid_r = std::max(1, std::min(b->ntiles_r, per_sm_r * b->sm_count));
@@ -2555,33 +2563,29 @@ ddhdg_batch_create(const ddhdg_batch_item *items, int n, int thermo, ddhdg_batch
         }
       else
         {
-          // the tables are read through L1 (not staged) and the chunk of
-          // trace columns is the largest that keeps two CTAs on an SM; R
-          // moves to global memory only when nothing else fits (neither
-          // choice changes the arithmetic)
-          int    chunk = 0;
-          bool   r_global = false;
-          size_t smem     = 0;
+          // the tables are read through L1 (not staged); R stays in shared
+          // memory if that keeps two CTAs on an SM, else if it fits at all,
+          // else it moves to global memory (no choice changes the arithmetic)
+          bool   found = false, r_global = false;
+          size_t smem  = 0;
           for (size_t limit : {(size_t)110 * 1024, (size_t)220 * 1024})
             {
-              for (int rg = 0; rg < 2 && !chunk; ++rg)
-                for (int ch = 16; ch >= 1 && !chunk; ch /= 2)
-                  {
-                    const Ws2Off w = ws2_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, ch, rg != 0);
-                    if ((size_t)w.total * sizeof(double) <= limit)
-                      {
-                        chunk    = ch;
-                        r_global = rg != 0;
-                        smem     = (size_t)w.total * sizeof(double);
-                      }
-                  }
-              if (chunk)
+              for (int rg = 0; rg < 2 && !found; ++rg)
+                {
+                  const Ws2Off w = ws2_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, rg != 0);
+                  if ((size_t)w.total * sizeof(double) <= limit)
+                    {
+                      found    = true;
+                      r_global = rg != 0;
+                      smem     = (size_t)w.total * sizeof(double);
+                    }
+                }
+              if (found)
                 break;
             }
-          if (!chunk)
+          if (!found)
             return fail(DDHDG_BAD_ARG, "the per-cell workspace does not fit in shared memory");
           J.P.wpb   = 1;
-          J.P.chunk = chunk;
           J.P.stage = 0;
           b->smem_c = std::max(b->smem_c, smem);
           if (r_global)
@@ -2821,7 +2825,10 @@ ddhdg_batch_autotune(ddhdg_batch *b, int reps, float *best_ms, ddhdg_stream_t st
           b->cells_per_tile[k] = keep;
         }
     }
-  for (int cps = 1; cps <= 2; ++cps)
+  // CTAs per SM: 1 up to what the kernel's registers and the batch's
+  // shared memory allow (at most 4)
+  b->ctas_per_sm = std::min(b->ctas_per_sm, b->occ_c);
+  for (int cps = 1; cps <= std::min(4, b->occ_c); ++cps)
     {
       if (cps == b->ctas_per_sm)
         continue;

@@ -37,11 +37,11 @@ namespace ddhdg
     int al, be, ka, ga, rh;             // per pair (9) coefficients
     int ctc, ctd, tcS, tcW, ttc, rhsf;  // per component / pair face data
     int r0, r1, rf;                     // residual coefficients
-    int S, R, g, dfl, rhsA, U, Wn, X, total;
+    int S, R, g, dfl, rhsA, total;
   };
 
   __host__ __device__ inline Ws2Off
-  ws2_layout(int dim, int nb, int nf, int ncomp, int ncol, int chunk, bool r_global = false)
+  ws2_layout(int dim, int nb, int nf, int ncomp, int ncol, bool r_global = false)
   {
     const int F = 2 * dim, nqc = nb, Fq = F * nf;
     const int Ns = ncomp * nb, Nt = F * ncomp * nf;
@@ -83,11 +83,234 @@ namespace ddhdg
     o.g     = take(Nt);
     o.dfl   = take(Nt);
     o.rhsA  = take(Nt);
-    o.U     = take(chunk * 3 * Fq);
-    o.Wn    = take(chunk * 3 * Fq);
-    o.X     = take(Nt * chunk);
     o.total = p;
     return o;
+  }
+
+  // D += A B for one 8x8x4 FP64 tile on the tensor path (mma.sync m8n8k4):
+  // lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}]
+  __device__ __forceinline__ void
+  cta_dmma8x8x4(double &d0, double &d1, double a, double b)
+  {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+  }
+
+  constexpr int CtaLuNB = 8; // panel width of the blocked LU
+
+  // The solve of the CTA-per-cell condensation: LU with partial pivoting of
+  // the row-equilibrated S (Ns x Ns, row stride ldS) applied to R (Ns x ncol,
+  // row stride ncol), then U Y = R' by block back substitution; R becomes Y.
+  // Right-looking, panels of CtaLuNB columns:
+  // - warp 0 factorises the panel (pivot search by a warp reduction over the
+  //   rows below the diagonal, row swaps and multipliers inside the panel);
+  // - the CTA, a thread per column, applies the panel's row swaps to the
+  //   columns right of it (S, then R) and solves the panel rows of U there
+  //   with the unit lower panel block;
+  // - the trailing update A22 -= L21 U12 runs on the FP64 tensor path in
+  //   8 x 8 tiles (K = the panel width), the warps taking tiles in turn.
+  // The pivots are those of the unblocked factorisation: each panel sees its
+  // columns fully updated.  The multipliers of finished panels are not
+  // swapped (nothing reads them again).  Back substitution per panel block
+  // from the bottom: the diagonal block a thread per column of R, then the
+  // rows above on the tensor path.  Three barriers per panel and two per
+  // block, against three and two per column unblocked.  Sets sh_sing when a
+  // pivot is zero or not finite.
+  template <int T>
+  __device__ void
+  cta_lu_solve(double *S, int ldS, double *R, int ncol, int Ns, int *sh_p, int &sh_sing)
+  {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = T / 32;
+    const int g = lane >> 2, q = lane & 3;
+    for (int j0 = 0; j0 < Ns; j0 += CtaLuNB)
+      {
+        const int w = min(CtaLuNB, Ns - j0);
+        // ---- panel: warp 0
+        if (warp == 0)
+          {
+            for (int jj = 0; jj < w; ++jj)
+              {
+                const int j    = j0 + jj;
+                double    best = -1.;
+                int       bi   = j;
+                for (int i = j + lane; i < Ns; i += 32)
+                  {
+                    const double v = fabs(S[i * ldS + j]);
+                    if (v > best)
+                      {
+                        best = v;
+                        bi   = i;
+                      }
+                  }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+                  {
+                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int    oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ob > best || (ob == best && oi < bi))
+                      {
+                        best = ob;
+                        bi   = oi;
+                      }
+                  }
+                if (lane == 0)
+                  {
+                    sh_p[jj] = bi;
+                    if (!(best > 0.) || !isfinite(best))
+                      sh_sing = 1;
+                  }
+                if (bi != j && lane < w)
+                  {
+                    const double t0          = S[j * ldS + j0 + lane];
+                    S[j * ldS + j0 + lane]  = S[bi * ldS + j0 + lane];
+                    S[bi * ldS + j0 + lane] = t0;
+                  }
+                __syncwarp();
+                const double d   = S[j * ldS + j];
+                const double inv = (d != 0.) ? 1. / d : 0.;
+                for (int i = j + 1 + lane; i < Ns; i += 32)
+                  {
+                    const double l = S[i * ldS + j] * inv;
+                    S[i * ldS + j] = l;
+                    for (int c = j + 1; c < j0 + w; ++c)
+                      S[i * ldS + c] -= l * S[j * ldS + c];
+                  }
+                __syncwarp();
+              }
+          }
+        __syncthreads();
+        // ---- swaps and U12 on the columns right of the panel: S, then R
+        const int nSr = Ns - j0 - w;
+        for (int v = tid; v < nSr + ncol; v += T)
+          {
+            double   *col = (v < nSr) ? S + j0 + w + v : R + (v - nSr);
+            const int ld  = (v < nSr) ? ldS : ncol;
+            double    x[CtaLuNB];
+#pragma unroll
+            for (int jj = 0; jj < CtaLuNB; ++jj)
+              if (jj < w)
+                {
+                  const int p = sh_p[jj], j = j0 + jj;
+                  if (p != j)
+                    {
+                      const double t0 = col[j * ld];
+                      col[j * ld]     = col[p * ld];
+                      col[p * ld]     = t0;
+                    }
+                }
+#pragma unroll
+            for (int jj = 0; jj < CtaLuNB; ++jj)
+              if (jj < w)
+                {
+                  double y = col[(j0 + jj) * ld];
+#pragma unroll
+                  for (int t = 0; t < CtaLuNB; ++t)
+                    if (t < jj)
+                      y -= S[(j0 + jj) * ldS + j0 + t] * x[t];
+                  x[jj] = y;
+                }
+#pragma unroll
+            for (int jj = 0; jj < CtaLuNB; ++jj)
+              if (jj < w)
+                col[(j0 + jj) * ld] = x[jj];
+          }
+        __syncthreads();
+        // ---- trailing update A22 -= L21 U12 (8 x 8 tiles on the tensor path)
+        const int r0 = j0 + w, nr = Ns - r0;
+        if (nr > 0)
+          {
+            const int nrt = (nr + 7) / 8, nct = (nSr + ncol + 7) / 8;
+            for (int tile = warp; tile < nrt * nct; tile += NW)
+              {
+                const int rt = tile % nrt, ct = tile / nrt;
+                const int row = r0 + rt * 8 + g;  // A-fragment row, D row
+                const int vb  = ct * 8 + g;       // B-fragment column
+                double    d0 = 0., d1 = 0.;
+#pragma unroll
+                for (int ks = 0; ks < CtaLuNB; ks += 4)
+                  {
+                    const int    k = ks + q;
+                    const double a = (k < w && row < Ns) ? S[row * ldS + j0 + k] : 0.;
+                    double       b = 0.;
+                    if (k < w && vb < nSr + ncol)
+                      b = (vb < nSr) ? S[(j0 + k) * ldS + r0 + vb] : R[(j0 + k) * ncol + vb - nSr];
+                    cta_dmma8x8x4(d0, d1, a, b);
+                  }
+                if (row < Ns)
+                  {
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+                      {
+                        const int    v  = ct * 8 + 2 * q + e;
+                        const double dv = e ? d1 : d0;
+                        if (v < nSr)
+                          S[row * ldS + r0 + v] -= dv;
+                        else if (v < nSr + ncol)
+                          R[row * ncol + v - nSr] -= dv;
+                      }
+                  }
+              }
+          }
+        __syncthreads();
+      }
+    // ---- back substitution U Y = R', blocks of the panels from the bottom
+    const int last = (Ns - 1) / CtaLuNB * CtaLuNB;
+    for (int j0 = last; j0 >= 0; j0 -= CtaLuNB)
+      {
+        const int w = min(CtaLuNB, Ns - j0);
+        for (int c = tid; c < ncol; c += T)
+          {
+            double y[CtaLuNB];
+#pragma unroll
+            for (int jj = CtaLuNB - 1; jj >= 0; --jj)
+              if (jj < w)
+                {
+                  double acc = R[(j0 + jj) * ncol + c];
+#pragma unroll
+                  for (int t = 0; t < CtaLuNB; ++t)
+                    if (t > jj && t < w)
+                      acc -= S[(j0 + jj) * ldS + j0 + t] * y[t];
+                  const double d = S[(j0 + jj) * ldS + j0 + jj];
+                  y[jj]          = acc * ((d != 0.) ? 1. / d : 0.);
+                }
+#pragma unroll
+            for (int jj = 0; jj < CtaLuNB; ++jj)
+              if (jj < w)
+                R[(j0 + jj) * ncol + c] = y[jj];
+          }
+        __syncthreads();
+        if (j0 > 0)
+          {
+            const int nrt = (j0 + 7) / 8, nct = (ncol + 7) / 8;
+            for (int tile = warp; tile < nrt * nct; tile += NW)
+              {
+                const int rt = tile % nrt, ct = tile / nrt;
+                const int row = rt * 8 + g, cb = ct * 8 + g;
+                double    d0 = 0., d1 = 0.;
+#pragma unroll
+                for (int ks = 0; ks < CtaLuNB; ks += 4)
+                  {
+                    const int    k = ks + q;
+                    const double a = (k < w && row < j0) ? S[row * ldS + j0 + k] : 0.;
+                    const double b = (k < w && cb < ncol) ? R[(j0 + k) * ncol + cb] : 0.;
+                    cta_dmma8x8x4(d0, d1, a, b);
+                  }
+                if (row < j0)
+                  {
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+                      {
+                        const int c = ct * 8 + 2 * q + e;
+                        if (c < ncol)
+                          R[row * ncol + c] -= e ? d1 : d0;
+                      }
+                  }
+              }
+            __syncthreads();
+          }
+      }
   }
 
   // The body of the CTA-per-cell condensation: the CTA (CondenseTPB threads)
@@ -110,7 +333,7 @@ namespace ddhdg
     constexpr int NCA = Dm::Nc_all;
     constexpr int T   = CondenseTPB;
     constexpr int NW  = T / 32;
-    __shared__ int sh_piv;
+    __shared__ int sh_p8[CtaLuNB];
     __shared__ int sh_sing;
 
     const int tid   = threadIdx.x;
@@ -121,7 +344,6 @@ namespace ddhdg
     const int Nt    = F * ncomp * nf;
     const int ncol  = P.ncol;
     const int ldS   = Ns + 1;
-    const int CH    = P.chunk;
     const bool two  = ncol > 1 + Nt;
 
     // ---- constant tables, staged once per CTA
@@ -150,7 +372,7 @@ namespace ddhdg
     const double *QW_c   = tb + P.to.QW_c;
     const double *QW_f   = tb + P.to.QW_f;
 
-    const Ws2Off wo = ws2_layout(DIM, nb, nf, ncomp, ncol, CH, P.rscratch != nullptr);
+    const Ws2Off wo = ws2_layout(DIM, nb, nf, ncomp, ncol, P.rscratch != nullptr);
     double *ws = smem + (P.stage ? ((P.to.total + 1) & ~1) : 0);
     double *coef = ws + wo.coef, *lam = ws + wo.lam, *c0 = ws + wo.c0, *W0 = ws + wo.W0,
            *qc = ws + wo.qc, *c0f = ws + wo.c0f, *W0n = ws + wo.W0n, *tr0 = ws + wo.tr0,
@@ -159,8 +381,7 @@ namespace ddhdg
            *rh = ws + wo.rh, *ctc = ws + wo.ctc, *ctd = ws + wo.ctd, *tcS = ws + wo.tcS,
            *tcW = ws + wo.tcW, *ttc = ws + wo.ttc, *rhsf = ws + wo.rhsf, *r0 = ws + wo.r0,
            *r1 = ws + wo.r1, *rf = ws + wo.rf, *S = ws + wo.S, *R = ws + wo.R,
-           *gv = ws + wo.g, *dfl = ws + wo.dfl, *rhsA = ws + wo.rhsA, *Ub = ws + wo.U,
-           *Wb = ws + wo.Wn, *Xc = ws + wo.X;
+           *gv = ws + wo.g, *dfl = ws + wo.dfl, *rhsA = ws + wo.rhsA;
     // R of the largest systems (3D k = 2 with drift columns: 210 KB) lives
     // in this CTA's slice of a global buffer, which stays in L2
     if (P.rscratch)
@@ -653,81 +874,7 @@ namespace ddhdg
               R[i * ncol + c] *= sc;
           }
         __syncthreads();
-        for (int j = 0; j < Ns; ++j)
-          {
-            if (warp == 0)
-              {
-                double best = -1.;
-                int    bi   = j;
-                for (int i = j + lane; i < Ns; i += 32)
-                  {
-                    const double v = fabs(S[i * ldS + j]);
-                    if (v > best)
-                      {
-                        best = v;
-                        bi   = i;
-                      }
-                  }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1)
-                  {
-                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                    const int    oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                    if (ob > best || (ob == best && oi < bi))
-                      {
-                        best = ob;
-                        bi   = oi;
-                      }
-                  }
-                if (lane == 0)
-                  {
-                    sh_piv = bi;
-                    if (!(best > 0.) || !isfinite(best))
-                      sh_sing = 1;
-                  }
-              }
-            __syncthreads();
-            const int p = sh_piv;
-            if (p != j)
-              {
-                for (int c = tid; c < Ns + ncol; c += T)
-                  {
-                    double *x  = (c < Ns) ? &S[j * ldS + c] : &R[j * ncol + c - Ns];
-                    double *y  = (c < Ns) ? &S[p * ldS + c] : &R[p * ncol + c - Ns];
-                    const double t0 = *x;
-                    *x              = *y;
-                    *y              = t0;
-                  }
-                __syncthreads();
-              }
-            const double piv = S[j * ldS + j];
-            const double inv = (piv != 0.) ? 1. / piv : 0.;
-            for (int i = j + 1 + warp; i < Ns; i += NW)
-              {
-                const double l = S[i * ldS + j] * inv;
-                for (int c = j + 1 + lane; c < Ns; c += 32)
-                  S[i * ldS + c] -= l * S[j * ldS + c];
-                for (int c = lane; c < ncol; c += 32)
-                  R[i * ncol + c] -= l * R[j * ncol + c];
-              }
-            __syncthreads();
-          }
-        // back substitution: R becomes Y
-        for (int j = Ns - 1; j >= 0; --j)
-          {
-            const double piv = S[j * ldS + j];
-            const double inv = (piv != 0.) ? 1. / piv : 0.;
-            for (int c = tid; c < ncol; c += T)
-              R[j * ncol + c] *= inv;
-            __syncthreads();
-            for (int i = warp; i < j; i += NW)
-              {
-                const double u = S[i * ldS + j];
-                for (int c = lane; c < ncol; c += 32)
-                  R[i * ncol + c] -= u * R[j * ncol + c];
-              }
-            __syncthreads();
-          }
+        cta_lu_solve<T>(S, ldS, R, ncol, Ns, sh_p8, sh_sing);
         if (tid == 0 && sh_sing)
           atomicExch(P.status, 3);
 
@@ -738,108 +885,116 @@ namespace ddhdg
             yc[idx] = R[(idx % Ns) * ncol + idx / Ns];
         }
 
-        // --------------------------- condensation on the faces, by chunks
-        for (int i = tid; i < Nt; i += T)
-          rhsA[i] = 0.;
-        double *tt_out = P.tt + cell * (int64_t)Nt * Nt;
-        for (int cbeg = 0; cbeg < 1 + Nt; cbeg += CH)
-          {
-            const int nch = min(CH, 1 + Nt - cbeg);
-            // scalar value and normal flux of every column on the faces
-            for (int idx = tid; idx < nch * ncomp * Fq; idx += T)
-              {
-                const int cc = idx / (ncomp * Fq);
-                const int r_ = idx % (ncomp * Fq);
-                const int ce = r_ / Fq, fq = r_ % Fq;
-                const int col = cbeg + cc;
-                double    u = 0., wn;
-                if (col == 0)
-                  wn = Wrf[ce * Fq + fq];
-                else
-                  {
-                    const int t = col - 1;
-                    const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
-                    wn = (ct == ce) ? RQr[fq * Ft + ft * nf + mt] : 0.;
-                  }
-                const bool add = two && col > 0;
+        // ---- tt = T Y + tc_W Q_t + face block, and the rows' rhs parts, on
+        // the FP64 tensor path.  T = tc_c + tc_W P (Nt x Ns: the trace rows'
+        // face integrals of the scalar values and normal fluxes) is formed
+        // on the fly as the A fragments; a warp takes 8 trace rows at a time
+        // against all 1 + Nt columns of Y (the residual column, then the
+        // trace columns with their drift columns added), and the epilogue
+        // adds the direct face terms: tc_W times the flux's own dependence
+        // on the residual (column 0) or on the trace (RQr), and the face
+        // block of tt.  The row's right-hand side part is the residual
+        // column minus the Dirichlet columns times their values, summed over
+        // the four lanes that hold the row.
+        {
+          constexpr int NTM    = F * 3 * nf;        // trace columns at most
+          constexpr int NNT    = (NTM + 8) / 8;     // column tiles of 1 + Nt columns
+          const int     g      = lane >> 2, tq = lane & 3;
+          double       *tt_out = P.tt + cell * (int64_t)Nt * Nt;
+          for (int m0 = warp * 8; m0 < Nt; m0 += NW * 8)
+            {
+              const int  i   = m0 + g;
+              const bool iok = i < Nt;
+              const int  ii  = iok ? i : 0;
+              const int  fi = ii / (ncomp * nf), ci = (ii / nf) % ncomp, mi = ii % nf;
+              const int  b  = P.comps[ci];
+              double     wrow[nqf];
 #pragma unroll
-                for (int e = 0; e < nb; ++e)
-                  {
-                    double y = R[(ce * nb + e) * ncol + col];
-                    if (add)
-                      y += R[(ce * nb + e) * ncol + col + Nt];
-                    u += phi_f[fq * nb + e] * y;
-                    wn += RTr[fq * nb + e] * y;
-                  }
-                Ub[(cc * 3 + ce) * Fq + fq] = u;
-                Wb[(cc * 3 + ce) * Fq + fq] = wn;
-              }
-            __syncthreads();
-            // combined trace-equation integrand -> Ub
-            for (int idx = tid; idx < nch * ncomp * Fq; idx += T)
-              {
-                const int cc = idx / (ncomp * Fq);
-                const int r_ = idx % (ncomp * Fq);
-                const int ce = r_ / Fq, fq = r_ % Fq;
-                const int b  = P.comps[ce];
-                double    v  = tcS[b * Fq + fq] * Ub[(cc * 3 + ce) * Fq + fq];
-                for (int cp = 0; cp < ncomp; ++cp)
-                  v += tcW[(b * 3 + P.comps[cp]) * Fq + fq] * Wb[(cc * 3 + cp) * Fq + fq];
-                Ub[(cc * 3 + ce) * Fq + fq] = v;
-              }
-            __syncthreads();
-            // tc X for every trace row and column of the chunk
-            for (int idx = tid; idx < Nt * nch; idx += T)
-              {
-                const int i = idx / nch, cc = idx % nch;
-                const int fi = i / (ncomp * nf), ci = (i / nf) % ncomp, mi = i % nf;
-                const int col = cbeg + cc;
-                double    x   = 0.;
+              for (int qf = 0; qf < nqf; ++qf)
+                wrow[qf] = w_f[fi * nqf + qf] * xi[qf * nf + mi];
+              double d[NNT][2];
 #pragma unroll
-                for (int qf = 0; qf < nqf; ++qf)
-                  x += w_f[fi * nqf + qf] * xi[qf * nf + mi] *
-                       Ub[(cc * 3 + ci) * Fq + fi * nqf + qf];
-                const bool rowD = dfl[i] != 0.;
-                Xc[i * CH + cc] = x;
-                if (col > 0)
+              for (int nt = 0; nt < NNT; ++nt)
+                d[nt][0] = d[nt][1] = 0.;
+              for (int k0 = 0; k0 < Ns; k0 += 4)
+                {
+                  const int j  = k0 + tq;
+                  double    av = 0.;
+                  if (iok && j < Ns)
+                    {
+                      const int     cj = j / nb, e = j % nb;
+                      const double *tw = tcW + (b * 3 + P.comps[cj]) * Fq + fi * nqf;
+                      const double *ts = tcS + b * Fq + fi * nqf;
+                      const bool    sc = cj == ci;
+#pragma unroll
+                      for (int qf = 0; qf < nqf; ++qf)
+                        {
+                          const int fq = fi * nqf + qf;
+                          av += wrow[qf] * (tw[qf] * RTr[fq * nb + e] + (sc ? ts[qf] * phi_f[fq * nb + e] : 0.));
+                        }
+                    }
+#pragma unroll
+                  for (int nt = 0; nt < NNT; ++nt)
+                    {
+                      const int col = nt * 8 + g; // B-fragment column
+                      double    bv  = 0.;
+                      if (j < Ns && col < 1 + Nt)
+                        {
+                          bv = R[j * ncol + col];
+                          if (two && col > 0)
+                            bv += R[j * ncol + col + Nt];
+                        }
+                      cta_dmma8x8x4(d[nt][0], d[nt][1], av, bv);
+                    }
+                }
+              const bool rok   = iok && dfl[ii] == 0.;
+              double     rpart = 0.;
+#pragma unroll
+              for (int nt = 0; nt < NNT; ++nt)
+#pragma unroll
+                for (int e = 0; e < 2; ++e)
                   {
-                    const int t = col - 1;
-                    double    o = 0.;
-                    if (dfl[t] == 0. && !rowD)
+                    const int col = nt * 8 + 2 * tq + e;
+                    if (!iok || col >= 1 + Nt)
+                      continue;
+                    double x = d[nt][e];
+                    if (col == 0)
                       {
-                        o              = x;
-                        const int ft   = t / (ncomp * nf);
-                        const int ct   = (t / nf) % ncomp;
-                        if (ft == fi && ct == ci)
-                          {
-                            const int b  = P.comps[ci];
-                            const int mt = t % nf;
 #pragma unroll
-                            for (int qf = 0; qf < nqf; ++qf)
-                              o += w_f[fi * nqf + qf] * ttc[b * Fq + fi * nqf + qf] *
-                                   xi[qf * nf + mi] * xi[qf * nf + mt];
-                          }
+                        for (int qf = 0; qf < nqf; ++qf)
+                          for (int cp = 0; cp < ncomp; ++cp)
+                            x += wrow[qf] * tcW[(b * 3 + P.comps[cp]) * Fq + fi * nqf + qf] *
+                                 Wrf[cp * Fq + fi * nqf + qf];
+                        rpart += x;
+                        continue;
+                      }
+                    const int t  = col - 1;
+                    const int ft = t / (ncomp * nf), ct = (t / nf) % ncomp, mt = t % nf;
+                    const double *tw = tcW + (b * 3 + P.comps[ct]) * Fq + fi * nqf;
+#pragma unroll
+                    for (int qf = 0; qf < nqf; ++qf)
+                      x += wrow[qf] * tw[qf] * RQr[(fi * nqf + qf) * Ft + ft * nf + mt];
+                    const bool cD = dfl[t] != 0.;
+                    if (cD)
+                      rpart -= x * gv[t];
+                    double o = 0.;
+                    if (rok && !cD)
+                      {
+                        o = x;
+                        if (ft == fi && ct == ci)
+#pragma unroll
+                          for (int qf = 0; qf < nqf; ++qf)
+                            o += wrow[qf] * ttc[b * Fq + fi * nqf + qf] * xi[qf * nf + mt];
                       }
                     tt_out[(int64_t)i * Nt + t] = o;
                   }
-              }
-            __syncthreads();
-            // residual column and Dirichlet columns -> rhs, in column order
-            for (int i = tid; i < Nt; i += T)
-              {
-                double acc = rhsA[i];
-                for (int cc = 0; cc < nch; ++cc)
-                  {
-                    const int col = cbeg + cc;
-                    if (col == 0)
-                      acc += Xc[i * CH + cc];
-                    else if (dfl[col - 1] != 0.)
-                      acc -= Xc[i * CH + cc] * gv[col - 1];
-                  }
-                rhsA[i] = acc;
-              }
-            __syncthreads();
-          }
+              rpart += __shfl_xor_sync(0xffffffffu, rpart, 1);
+              rpart += __shfl_xor_sync(0xffffffffu, rpart, 2);
+              if (iok && tq == 0)
+                rhsA[i] = rpart;
+            }
+        }
+        __syncthreads();
 
         // ------------------------------------- right-hand side and flags
         for (int i = tid; i < Nt; i += T)

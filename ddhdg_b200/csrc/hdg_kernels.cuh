@@ -45,7 +45,6 @@ namespace ddhdg
     int ncol;  // columns of the scalar system: 1 + Nt (+ Nt)
     int ycols; // columns kept for the reconstruction: 1 + Nt
     int wpb;   // warps per block
-    int chunk; // columns per chunk in the condensation stage
     int stage; // 1: copy the tables to shared memory, 0: read them from L1/L2
     // state
     const double *cell_state, *trace_state;

@@ -1063,10 +1063,23 @@ namespace ddhdg
 
     // Device bytes that build() allocates for the planned mesh: fronts,
     // pivots, inverted diagonal blocks, the maps and the scaling vectors,
-    // each allocation rounded up to the allocator's 2 MiB granularity, plus
-    // a bound of 64 nE doubles per side stream for the LU workspace of the
+    // each allocation rounded up to the allocator's 2 MiB granularity, a
+    // bound of 64 nE doubles per side stream for the LU workspace of the
     // largest front (the library reports its size only once a handle
-    // exists).  The caller's plan() must have succeeded.
+    // exists), and the library handles.  The caller's plan() must have
+    // succeeded.
+    // side streams (each with its library handles) that the plan's large
+    // fronts use: one per front of the largest per-front batch, at most NSide
+    int
+    side_count() const
+    {
+      int n = 0;
+      for (const auto &bt : batches_)
+        if (bt.big)
+          n = std::max(n, (int)bt.nodes.size());
+      return std::min(n, NSide);
+    }
+
     int64_t
     planned_device_bytes() const
     {
@@ -1097,7 +1110,11 @@ namespace ddhdg
       const int64_t ndofs = M_.nfaces * (int64_t)M_.nd;
       add(ndofs * 8);
       add(ndofs * 8);
-      add((int64_t)NSide * 64 * big_nE * 8);
+      add((int64_t)side_count() * 64 * big_nE * 8);
+      // library handles: one cuBLAS handle, and a cuBLAS and a cuSOLVER
+      // handle per side stream (measured on CUDA 12.9: about 70 MB and
+      // 300 MB of device memory each)
+      b += (int64_t)(1 + side_count()) * (80 << 20) + (int64_t)side_count() * (320 << 20);
       return b;
     }
 
@@ -1381,28 +1398,15 @@ namespace ddhdg
         return r;
       if (cublasCreate(&blas_) != CUBLAS_STATUS_SUCCESS)
         return bad(err, "cublasCreate failed", DDHDG_SOLVER_ERROR);
-      if (cusolverDnCreate(&dn_) != CUSOLVER_STATUS_SUCCESS)
-        return bad(err, "cusolverDnCreate failed", DDHDG_SOLVER_ERROR);
-      int64_t big_ws = 0;
-      for (auto &b : batches_)
-        if (b.big)
-          for (int id : b.nodes)
-            {
-              int       lw = 0;
-              const int nF = b.nE + b.nK;
-              if (cusolverDnDgetrf_bufferSize(dn_, b.nE, b.nE, d_fronts_ + nodes_[id].off, nF, &lw) !=
-                  CUSOLVER_STATUS_SUCCESS)
-                return bad(err, "cusolverDnDgetrf_bufferSize failed", DDHDG_SOLVER_ERROR);
-              big_ws = std::max<int64_t>(big_ws, lw);
-            }
-      work_per_ = std::max<int64_t>(big_ws, 1);
-      if ((r = dmalloc(d_work_, NSide * work_per_ * sizeof(double), err)))
-        return r;
+      // side streams with their own handles, only as many as the largest
+      // per-front batch uses (a cuSOLVER handle holds about 300 MB of device
+      // memory, a cuBLAS one about 70 MB)
+      nside_ = side_count();
       if (cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming) != cudaSuccess)
         return bad(err, "cudaEventCreate failed", DDHDG_CUDA_ERROR);
       if (cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking) != cudaSuccess)
         return bad(err, "cudaStreamCreate failed", DDHDG_CUDA_ERROR);
-      for (int k = 0; k < NSide; ++k)
+      for (int k = 0; k < nside_; ++k)
         {
           if (cudaStreamCreateWithFlags(&side_[k], cudaStreamNonBlocking) != cudaSuccess ||
               cudaEventCreateWithFlags(&ev_join_[k], cudaEventDisableTiming) != cudaSuccess)
@@ -1413,6 +1417,21 @@ namespace ddhdg
           cublasSetStream(side_blas_[k], side_[k]);
           cusolverDnSetStream(side_dn_[k], side_[k]);
         }
+      int64_t big_ws = 0;
+      for (auto &b : batches_)
+        if (b.big)
+          for (int id : b.nodes)
+            {
+              int       lw = 0;
+              const int nF = b.nE + b.nK;
+              if (cusolverDnDgetrf_bufferSize(side_dn_[0], b.nE, b.nE, d_fronts_ + nodes_[id].off, nF, &lw) !=
+                  CUSOLVER_STATUS_SUCCESS)
+                return bad(err, "cusolverDnDgetrf_bufferSize failed", DDHDG_SOLVER_ERROR);
+              big_ws = std::max<int64_t>(big_ws, lw);
+            }
+      work_per_ = std::max<int64_t>(big_ws, 1);
+      if ((r = dmalloc(d_work_, std::max(nside_, 1) * work_per_ * sizeof(double), err)))
+        return r;
       if (allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_front_kernel)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_front_capped_kernel<4>)) != cudaSuccess ||
           allow_full_dynamic_smem(reinterpret_cast<const void *>(nd_small_front_capped_kernel<5>)) != cudaSuccess ||
@@ -1522,7 +1541,6 @@ namespace ddhdg
       const int64_t ndofs = M.nfaces * (int64_t)M.nd;
       const int     grid  = sm_count * 8;
       cublasSetStream(blas_, s);
-      cusolverDnSetStream(dn_, s);
       // row equilibration
       if (cudaMemsetAsync(d_dmax_, 0, ndofs * sizeof(unsigned long long), s) != cudaSuccess)
         return bad(err, "memset failed", DDHDG_CUDA_ERROR);
@@ -1698,14 +1716,14 @@ namespace ddhdg
       const int nb = (int)b.nodes.size();
       if (cudaEventRecord(ev_fork_, s) != cudaSuccess)
         return bad(err, "cudaEventRecord failed", DDHDG_CUDA_ERROR);
-      const int used = std::min(nb, NSide);
+      const int used = std::min(nb, nside_);
       for (int k = 0; k < used; ++k)
         if (cudaStreamWaitEvent(side_[k], ev_fork_, 0) != cudaSuccess)
           return bad(err, "cudaStreamWaitEvent failed", DDHDG_CUDA_ERROR);
       const double one = 1., mone = -1.;
       for (int q = 0; q < nb; ++q)
         {
-          const int    k   = q % NSide;
+          const int    k   = q % nside_;
           cudaStream_t ss  = side_[k];
           double      *Fq  = d_fronts_ + nodes_[b.nodes[q]].off;
           int         *piv = d_piv_ + b.piv_off + (int64_t)q * b.nE;
@@ -1953,10 +1971,7 @@ namespace ddhdg
       allocs_.clear();
       if (blas_)
         cublasDestroy(blas_);
-      if (dn_)
-        cusolverDnDestroy(dn_);
       blas_  = nullptr;
-      dn_    = nullptr;
       for (int k = 0; k < NSide; ++k)
         {
           if (side_blas_[k])
@@ -2079,7 +2094,7 @@ namespace ddhdg
     NDSol              *d_sol_   = nullptr;
     unsigned long long *d_dmax_  = nullptr;
     cublasHandle_t      blas_    = nullptr;
-    cusolverDnHandle_t  dn_      = nullptr;
+    int                 nside_            = 0; // side streams created (side_count())
     cudaStream_t        side_[NSide]      = {};
     cublasHandle_t      side_blas_[NSide] = {};
     cusolverDnHandle_t  side_dn_[NSide]   = {};

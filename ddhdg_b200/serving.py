@@ -75,16 +75,16 @@ def trace_solver_bytes(dim: int, m: int, k: int, ncomp: int) -> int:
     return int(out.value)
 
 
-# Device bytes of one request beyond its arrays: the library handles of the
-# trace solver's side streams (two modes), its CUDA graphs and the context's
-# streams and events
-REQUEST_OVERHEAD = 1 << 30
+# Device bytes of one request beyond its arrays and its trace solver (whose
+# library handles trace_solver_bytes counts): CUDA graphs, the context's and
+# the batch's streams and events
+REQUEST_OVERHEAD = 256 << 20
 
 
 def memory_estimate(dim: int, m: int, k: int) -> int:
-    """Device bytes of one solve: the trace solvers of both phases (the
-    biased system and the V-only equilibrium system, which stays allocated
-    for the rest of the solve) from their plans, the global trace sparsity,
+    """Device bytes of one solve: the larger of the two phases' trace
+    solvers (the V-only equilibrium system's is released before the biased
+    system's is built) from their plans, the global trace sparsity,
     the per-cell states, condensed blocks and Y cache of both phases, and the
     per-request overhead; the array terms 10 % over."""
     nb = (k + 1) ** dim
@@ -96,7 +96,7 @@ def memory_estimate(dim: int, m: int, k: int) -> int:
     per_cell = 8 * (3 * (dim + 1) * nb * 3 + Nt * Nt + 3 * Nt + Ns * (1 + Nt))
     # the batched launch keeps its own Y cache of the request's cells
     batch_y = 8 * Ns * (1 + Nt)
-    fronts = trace_solver_bytes(dim, m, k, 3) + trace_solver_bytes(dim, m, k, 1)
+    fronts = max(trace_solver_bytes(dim, m, k, 3), trace_solver_bytes(dim, m, k, 1))
     # the global trace sparsity of both modes (values, column indices and
     # the permutation maps: about 20 bytes per nonzero; a face couples to
     # the 4 dim - 1 faces of its two cells)
@@ -135,7 +135,7 @@ def request_precision(req: Request, mixed: bool) -> int:
 
 def solve_one(req: Request, device="cuda:0", keep_state=False, tol=1e-10, max_it=50, mixed=False):
     """One request's solve on the calling thread's current CUDA stream."""
-    from . import workloads
+    from . import _lib, workloads
     from .solver import NPSolver
 
     pb, prm, adim = workloads.diode(dim=req.dim, m=req.m, k=req.k, precision=request_precision(req, mixed))
@@ -144,6 +144,8 @@ def solve_one(req: Request, device="cuda:0", keep_state=False, tol=1e-10, max_it
     g = NPSolver(pb, prm, adim, device=device)
     res = g.compute_thermodynamic_equilibrium()
     it = res.iterations
+    # the equilibrium system's trace solver is not used again
+    _lib.check(g.L.ddhdg_release_solver(g._ctx, 1), "release_solver")
     if req.bias != 0.0:
         workloads.set_bias(pb, req.bias)
         g.update_boundary_tables()
@@ -344,6 +346,9 @@ class DiodeServer(ThreadedDiodeServer):
             for c in (1, 2):
                 _lib.check(g.L.ddhdg_project_density(g._ctx, c, 0.0, g.cell_state.data_ptr(),
                                                      g.trace_state.data_ptr(), g._sp()), "project_density")
+            # the equilibrium system's trace solver is not used again: its
+            # fronts go back before the biased system's solver is built
+            _lib.check(g.L.ddhdg_release_solver(g._ctx, 1), "release_solver")
             if a.req.bias != 0.0:
                 workloads.set_bias(a.problem, a.req.bias)
                 g.update_boundary_tables()

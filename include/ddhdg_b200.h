@@ -250,6 +250,14 @@ int ddhdg_solve_condensed(ddhdg_ctx *ctx, const double *tt, const double *rhs,
  * that make only a couple of solves per context.  Both give the same bits. */
 int ddhdg_set_solver_graphs(ddhdg_ctx *ctx, int enable);
 
+/* No counterpart in the reference.  Frees the trace solver of one mode
+ * (thermo_eq 0: the full system, 1: the equilibrium system): its fronts,
+ * library handles, side streams and graphs.  The next solve of that mode
+ * builds it again (the host plan comes from the process-wide cache).  A
+ * serving loop calls it when a request leaves the equilibrium phase.
+ * Synchronises the device first. */
+int ddhdg_release_solver(ddhdg_ctx *ctx, int thermo_eq);
+
 /* No counterpart in the reference (its solve is UMFPACK or GMRES on the
  * host).  Device bytes that the trace solver of a structured mesh allocates
  * (fronts, pivots, maps), from its host-side plan alone: `dim`, cells per
