@@ -32,6 +32,7 @@ EXPORTS = [
     "ddhdg_reconstruct_plain", "ddhdg_sample_points", "ddhdg_batch_create", "ddhdg_batch_destroy",
     "ddhdg_batch_condense", "ddhdg_batch_reconstruct", "ddhdg_batch_set_shape", "ddhdg_batch_get_shape",
     "ddhdg_batch_autotune", "ddhdg_batch_newton_step", "ddhdg_trace_solver_bytes", "ddhdg_release_solver",
+    "ddhdg_batch_newton_step_begin", "ddhdg_batch_newton_step_end",
 ]
 
 
@@ -121,6 +122,8 @@ def load(build_if_missing: bool = True):
     L.ddhdg_batch_get_shape.argtypes = [c_void_p, P(c_int), P(c_int), P(c_int), P(c_int)]
     L.ddhdg_batch_autotune.argtypes = [c_void_p, c_int, P(ctypes.c_float), c_void_p]
     L.ddhdg_batch_newton_step.argtypes = [c_void_p, dp, dp, P(c_int), c_void_p]
+    L.ddhdg_batch_newton_step_begin.argtypes = [c_void_p, dp, c_void_p]
+    L.ddhdg_batch_newton_step_end.argtypes = [c_void_p, c_int, dp, P(c_int), P(c_int)]
     L.ddhdg_newton.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_double, c_double, c_int,
                                c_double, P(c_int), P(c_double), c_void_p]
     L.ddhdg_last_timings.argtypes = [c_void_p, P(c_double), P(c_double), P(c_double), P(c_int)]

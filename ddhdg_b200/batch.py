@@ -98,6 +98,36 @@ class CondenseBatch:
             _lib.check(code, "batch_newton_step")
         return norms, list(status)
 
+    def newton_step_begin(self, alphas):
+        """Enqueue one Newton step of every solver (as ``newton_step``) and
+        return at once."""
+        import numpy as np
+
+        n = len(self.solvers)
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(alphas, dtype=np.float64), (n,)))
+        dp = ctypes.POINTER(ctypes.c_double)
+        _lib.check(self.L.ddhdg_batch_newton_step_begin(self._b, a.ctypes.data_as(dp), self._sp()),
+                   "batch_newton_step_begin")
+
+    def newton_step_end(self, wait=True):
+        """The result of the step in flight: (norms, statuses) as
+        ``newton_step`` returns them, or None while it is still running
+        (wait=False)."""
+        import numpy as np
+
+        n = len(self.solvers)
+        norms = np.zeros((n, 4))
+        status = (ctypes.c_int * n)()
+        done = ctypes.c_int()
+        dp = ctypes.POINTER(ctypes.c_double)
+        code = self.L.ddhdg_batch_newton_step_end(self._b, int(bool(wait)), norms.ctypes.data_as(dp), status,
+                                                  ctypes.byref(done))
+        if code not in (0, 3, 8):
+            _lib.check(code, "batch_newton_step_end")
+        if not done.value:
+            return None
+        return norms, list(status)
+
     def condense(self):
         _lib.check(self.L.ddhdg_batch_condense(self._b, self._sp()), "batch_condense")
 

@@ -2243,8 +2243,23 @@ struct ddhdg_batch
   DevBuf<unsigned long long> norms;
   cudaStream_t             side[NS] = {};
   cudaEvent_t              ev_fork = nullptr, ev_join[NS] = {};
+  // a step begun and not yet ended: its stream, its completion event and
+  // the pinned host copies of its norms and statuses
+  bool                     pending  = false;
+  cudaStream_t             step_s   = nullptr;
+  cudaEvent_t              ev_done  = nullptr;
+  double                  *h_norms  = nullptr;
+  int                     *h_status = nullptr;
   ~ddhdg_batch()
   {
+    if (pending && ev_done)
+      cudaEventSynchronize(ev_done);
+    if (ev_done)
+      cudaEventDestroy(ev_done);
+    if (h_norms)
+      cudaFreeHost(h_norms);
+    if (h_status)
+      cudaFreeHost(h_status);
     for (auto &st : side)
       if (st)
         cudaStreamDestroy(st);
@@ -2644,11 +2659,12 @@ ddhdg_batch_reconstruct(ddhdg_batch *b, ddhdg_stream_t stream)
 }
 
 int
-ddhdg_batch_newton_step(ddhdg_batch *b, const double *alpha, double *norms_host, int *status_host,
-                        ddhdg_stream_t stream)
+ddhdg_batch_newton_step_begin(ddhdg_batch *b, const double *alpha, ddhdg_stream_t stream)
 {
-  if (!b || !alpha || !norms_host)
+  if (!b || !alpha)
     return fail(DDHDG_BAD_ARG, "null argument");
+  if (b->pending)
+    return fail(DDHDG_BAD_ARG, "the batch has a step that has not ended");
   for (const auto &J : b->jobs)
     if (!J.dtrace || !J.dcell)
       return fail(DDHDG_BAD_ARG, "a batch item has no update_trace / update_cell");
@@ -2677,6 +2693,9 @@ ddhdg_batch_newton_step(ddhdg_batch *b, const double *alpha, double *norms_host,
           CK(cudaEventCreateWithFlags(&b->ev_join[k], cudaEventDisableTiming));
         }
       CK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming));
+      CK(cudaMallocHost(reinterpret_cast<void **>(&b->h_norms), (size_t)4 * n * sizeof(double)));
+      CK(cudaMallocHost(reinterpret_cast<void **>(&b->h_status), (size_t)n * sizeof(int)));
     }
   for (int i = 0; i < n; ++i)
     CK(cudaMemsetAsync(b->ctx[i]->status.p, 0, sizeof(int), s));
@@ -2728,11 +2747,37 @@ ddhdg_batch_newton_step(ddhdg_batch *b, const double *alpha, double *norms_host,
                                                                alpha[i]);
     }
   CK(cudaGetLastError());
-  std::vector<int> st(n, 0);
-  CK(cudaMemcpyAsync(norms_host, b->norms.p, (size_t)4 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(b->h_norms, b->norms.p, (size_t)4 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   for (int i = 0; i < n; ++i)
-    CK(cudaMemcpyAsync(&st[i], b->ctx[i]->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpyAsync(b->h_status + i, b->ctx[i]->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaEventRecord(b->ev_done, s));
+  b->step_s  = s;
+  b->pending = true;
+  return DDHDG_OK;
+}
+
+int
+ddhdg_batch_newton_step_end(ddhdg_batch *b, int wait, double *norms_host, int *status_host, int *done)
+{
+  if (!b || !norms_host || !done)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  *done = 0;
+  if (!b->pending)
+    return fail(DDHDG_BAD_ARG, "the batch has no step in flight");
+  if (!wait)
+    {
+      const cudaError_t q = cudaEventQuery(b->ev_done);
+      if (q == cudaErrorNotReady)
+        return DDHDG_OK;
+      if (q != cudaSuccess)
+        return fail(DDHDG_CUDA_ERROR, cudaGetErrorString(q));
+    }
+  else
+    CK(cudaEventSynchronize(b->ev_done));
+  b->pending = false;
+  *done      = 1;
+  const int n = b->n;
+  std::memcpy(norms_host, b->h_norms, (size_t)4 * n * sizeof(double));
   // singular fronts of the trace solves (their pivot status, read now)
   int worst = DDHDG_OK;
   for (int i = 0; i < n; ++i)
@@ -2740,16 +2785,29 @@ ddhdg_batch_newton_step(ddhdg_batch *b, const double *alpha, double *norms_host,
       ddhdg_ctx  *c  = b->ctx[i];
       NDSolver   *nd = nullptr;
       std::string err;
-      if (nd_solver(c, c->mode[b->thermo], nd) == DDHDG_OK && nd->check_info(s, err) != DDHDG_OK)
-        st[i] = DDHDG_SOLVER_ERROR;
+      int         st = b->h_status[i];
+      if (nd_solver(c, c->mode[b->thermo], nd) == DDHDG_OK && nd->check_info(b->step_s, err) != DDHDG_OK)
+        st = DDHDG_SOLVER_ERROR;
       if (status_host)
-        status_host[i] = st[i];
-      if (st[i] && !worst)
-        worst = st[i];
+        status_host[i] = st;
+      if (st && !worst)
+        worst = st;
     }
   if (worst)
     return fail(worst, "a batch item had a singular local system or trace front (see the item statuses)");
   return DDHDG_OK;
+}
+
+int
+ddhdg_batch_newton_step(ddhdg_batch *b, const double *alpha, double *norms_host, int *status_host,
+                        ddhdg_stream_t stream)
+{
+  if (!b || !alpha || !norms_host)
+    return fail(DDHDG_BAD_ARG, "null argument");
+  int r, done = 0;
+  if ((r = ddhdg_batch_newton_step_begin(b, alpha, stream)))
+    return r;
+  return ddhdg_batch_newton_step_end(b, 1, norms_host, status_host, &done);
 }
 
 int

@@ -103,8 +103,9 @@ namespace ddhdg
   // the row-equilibrated S (Ns x Ns, row stride ldS) applied to R (Ns x ncol,
   // row stride ncol), then U Y = R' by block back substitution; R becomes Y.
   // Right-looking, panels of CtaLuNB columns:
-  // - warp 0 factorises the panel (pivot search by a warp reduction over the
-  //   rows below the diagonal, row swaps and multipliers inside the panel);
+  // - warp 0 factorises the panel with its rows in registers (pivot search
+  //   by a warp reduction over the rows below the diagonal, the pivot row
+  //   exchanged and broadcast by shuffles, multipliers inside the panel);
   // - the CTA, a thread per column, applies the panel's row swaps to the
   //   columns right of it (S, then R) and solves the panel rows of U there
   //   with the unit lower panel block;
@@ -117,31 +118,48 @@ namespace ddhdg
   // rows above on the tensor path.  Three barriers per panel and two per
   // block, against three and two per column unblocked.  Sets sh_sing when a
   // pivot is zero or not finite.
-  template <int T>
+  // NSMAX: the largest Ns (rows of the panel held per lane: NSMAX / 32,
+  // rounded up)
+  template <int T, int NSMAX>
   __device__ void
   cta_lu_solve(double *S, int ldS, double *R, int ncol, int Ns, int *sh_p, int &sh_sing)
   {
+    constexpr int PR = (NSMAX + 31) / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = T / 32;
     const int g = lane >> 2, q = lane & 3;
     for (int j0 = 0; j0 < Ns; j0 += CtaLuNB)
       {
         const int w = min(CtaLuNB, Ns - j0);
-        // ---- panel: warp 0
+        // ---- panel: warp 0, its rows in registers (lane l holds rows
+        // j0 + l + 32 r), pivot rows exchanged and broadcast by shuffles
         if (warp == 0)
           {
-            for (int jj = 0; jj < w; ++jj)
+            double v[PR][CtaLuNB];
+#pragma unroll
+            for (int r = 0; r < PR; ++r)
               {
+                const int row = j0 + lane + 32 * r;
+#pragma unroll
+                for (int c = 0; c < CtaLuNB; ++c)
+                  v[r][c] = (row < Ns && c < w) ? S[row * ldS + j0 + c] : 0.;
+              }
+#pragma unroll
+            for (int jj = 0; jj < CtaLuNB; ++jj)
+              {
+                if (jj >= w)
+                  break;
                 const int j    = j0 + jj;
                 double    best = -1.;
-                int       bi   = j;
-                for (int i = j + lane; i < Ns; i += 32)
+                int       bi   = Ns;
+#pragma unroll
+                for (int r = 0; r < PR; ++r)
                   {
-                    const double v = fabs(S[i * ldS + j]);
-                    if (v > best)
+                    const int row = j0 + lane + 32 * r;
+                    if (row >= j && row < Ns && fabs(v[r][jj]) > best)
                       {
-                        best = v;
-                        bi   = i;
+                        best = fabs(v[r][jj]);
+                        bi   = row;
                       }
                   }
 #pragma unroll
@@ -155,29 +173,76 @@ namespace ddhdg
                         bi   = oi;
                       }
                   }
+                if (bi >= Ns)
+                  bi = j; // no finite candidate: keep the row (singular)
                 if (lane == 0)
                   {
                     sh_p[jj] = bi;
                     if (!(best > 0.) || !isfinite(best))
                       sh_sing = 1;
                   }
-                if (bi != j && lane < w)
+                const int oj = (j - j0) & 31, sj = (j - j0) >> 5;
+                if (bi != j)
                   {
-                    const double t0          = S[j * ldS + j0 + lane];
-                    S[j * ldS + j0 + lane]  = S[bi * ldS + j0 + lane];
-                    S[bi * ldS + j0 + lane] = t0;
+                    const int op = (bi - j0) & 31, sp = (bi - j0) >> 5;
+#pragma unroll
+                    for (int c = 0; c < CtaLuNB; ++c)
+                      {
+                        double xp = 0., xj = 0.;
+#pragma unroll
+                        for (int r = 0; r < PR; ++r)
+                          {
+                            xp = (r == sp) ? v[r][c] : xp;
+                            xj = (r == sj) ? v[r][c] : xj;
+                          }
+                        xp = __shfl_sync(0xffffffffu, xp, op);
+                        xj = __shfl_sync(0xffffffffu, xj, oj);
+#pragma unroll
+                        for (int r = 0; r < PR; ++r)
+                          {
+                            if (lane == oj && r == sj)
+                              v[r][c] = xp;
+                            if (lane == op && r == sp)
+                              v[r][c] = xj;
+                          }
+                      }
                   }
-                __syncwarp();
-                const double d   = S[j * ldS + j];
+                double prow[CtaLuNB];
+#pragma unroll
+                for (int c = 0; c < CtaLuNB; ++c)
+                  {
+                    double x = 0.;
+#pragma unroll
+                    for (int r = 0; r < PR; ++r)
+                      x = (r == sj) ? v[r][c] : x;
+                    prow[c] = __shfl_sync(0xffffffffu, x, oj);
+                  }
+                const double d   = prow[jj];
                 const double inv = (d != 0.) ? 1. / d : 0.;
-                for (int i = j + 1 + lane; i < Ns; i += 32)
+#pragma unroll
+                for (int r = 0; r < PR; ++r)
                   {
-                    const double l = S[i * ldS + j] * inv;
-                    S[i * ldS + j] = l;
-                    for (int c = j + 1; c < j0 + w; ++c)
-                      S[i * ldS + c] -= l * S[j * ldS + c];
+                    const int row = j0 + lane + 32 * r;
+                    if (row > j && row < Ns)
+                      {
+                        const double l = v[r][jj] * inv;
+                        v[r][jj]       = l;
+#pragma unroll
+                        for (int c = jj + 1; c < CtaLuNB; ++c)
+                          if (c < w)
+                            v[r][c] -= l * prow[c];
+                      }
                   }
-                __syncwarp();
+              }
+#pragma unroll
+            for (int r = 0; r < PR; ++r)
+              {
+                const int row = j0 + lane + 32 * r;
+                if (row < Ns)
+#pragma unroll
+                  for (int c = 0; c < CtaLuNB; ++c)
+                    if (c < w)
+                      S[row * ldS + j0 + c] = v[r][c];
               }
           }
         __syncthreads();
@@ -874,7 +939,7 @@ namespace ddhdg
               R[i * ncol + c] *= sc;
           }
         __syncthreads();
-        cta_lu_solve<T>(S, ldS, R, ncol, Ns, sh_p8, sh_sing);
+        cta_lu_solve<T, 3 * nb>(S, ldS, R, ncol, Ns, sh_p8, sh_sing);
         if (tid == 0 && sh_sing)
           atomicExch(P.status, 3);
 

@@ -82,9 +82,10 @@ REQUEST_OVERHEAD = 256 << 20
 
 
 def memory_estimate(dim: int, m: int, k: int) -> int:
-    """Device bytes of one solve: the larger of the two phases' trace
-    solvers (the V-only equilibrium system's is released before the biased
-    system's is built) from their plans, the global trace sparsity,
+    """Device bytes of one solve: the trace solvers of both phases (the
+    V-only equilibrium system's is released only when no step is in flight,
+    so it may still be held while the biased system's is built) from their
+    plans, the global trace sparsity,
     the per-cell states, condensed blocks and Y cache of both phases, and the
     per-request overhead; the array terms 10 % over."""
     nb = (k + 1) ** dim
@@ -96,7 +97,7 @@ def memory_estimate(dim: int, m: int, k: int) -> int:
     per_cell = 8 * (3 * (dim + 1) * nb * 3 + Nt * Nt + 3 * Nt + Ns * (1 + Nt))
     # the batched launch keeps its own Y cache of the request's cells
     batch_y = 8 * Ns * (1 + Nt)
-    fronts = max(trace_solver_bytes(dim, m, k, 3), trace_solver_bytes(dim, m, k, 1))
+    fronts = trace_solver_bytes(dim, m, k, 3) + trace_solver_bytes(dim, m, k, 1)
     # the global trace sparsity of both modes (values, column indices and
     # the permutation maps: about 20 bytes per nonzero; a face couples to
     # the 4 dim - 1 faces of its two cells)
@@ -297,26 +298,54 @@ class _Active:
         self.buffers = {}
 
 
+class _Deferred:
+    """Device memory handed back when no step is in flight: a cudaFree
+    waits for the whole device, so the server does not free while other
+    requests' steps run (unless an arrival needs the memory)."""
+
+    def __init__(self, fn):
+        self.fn = fn
+
+    def close(self):
+        fn, self.fn = self.fn, None
+        if fn is not None:
+            fn()
+
+
 class DiodeServer(ThreadedDiodeServer):
     """Continuous batching of diode solves on one GPU, at kernel level.
 
-    Every server step advances each request in flight by one Newton step:
-    one batched condensation launch over all requests of a phase, their trace
-    solves overlapped on side streams, one batched reconstruction launch and
-    the damped updates (``CondenseBatch.newton_step``).  The loop is
-    ``private_run`` (src/np_solver.cpp:1452-1561) per request: the stopping
-    rule on the update and state norms and the damping are the solver's.
-    Arrivals join at the next step once a slot and their device memory are
-    free; converged requests leave.  Memory admission as in
-    ``ThreadedDiodeServer``."""
+    The requests in flight form groups by (phase, dimension, size class);
+    each group advances by one Newton step at a time: one batched
+    condensation launch over its requests, their trace solves overlapped on
+    side streams, one batched reconstruction launch and the damped updates
+    (``CondenseBatch.newton_step_begin`` / ``newton_step_end``).  Groups step
+    independently, each on its own stream: the host loop begins the step of
+    every idle group, then collects the steps that have ended, so a group of
+    small requests is not held back by the long trace solves of a group of
+    large ones.  The loop is ``private_run`` (src/np_solver.cpp:1452-1561)
+    per request: the stopping rule on the update and state norms and the
+    damping are the solver's.  Arrivals join their group at its next step
+    once a slot and their device memory are free; converged requests leave.
+    Memory admission as in ``ThreadedDiodeServer``; memory of finished
+    requests and replaced batches goes back when no step is in flight or
+    when an arrival needs it.
+
+    big_bytes: requests whose memory estimate exceeds it form their own
+    groups (the large class)."""
 
     def __init__(self, max_inflight=16, hbm_reserve=4 << 30, hbm_limit=None, device="cuda:0",
-                 keep_states=False, mem_info=None, tol=1e-10, max_it=50, mixed=False):
+                 keep_states=False, mem_info=None, tol=1e-10, max_it=50, mixed=False, big_bytes=8 << 30):
         super().__init__(max_inflight, hbm_reserve, hbm_limit, device, keep_states, mem_info, mixed)
         self.tol = tol
         self.max_it = max_it
-        self.steps = 0
+        self.big_bytes = big_bytes
+        self.steps = 0  # group steps
         self.peak_batch = 0
+        self._deferred = []
+
+    def _group_key(self, a):
+        return (a.phase, a.req.dim, 1 if a.est > self.big_bytes else 0)
 
     def _start_request(self, a):
         from . import workloads
@@ -347,8 +376,9 @@ class DiodeServer(ThreadedDiodeServer):
                 _lib.check(g.L.ddhdg_project_density(g._ctx, c, 0.0, g.cell_state.data_ptr(),
                                                      g.trace_state.data_ptr(), g._sp()), "project_density")
             # the equilibrium system's trace solver is not used again: its
-            # fronts go back before the biased system's solver is built
-            _lib.check(g.L.ddhdg_release_solver(g._ctx, 1), "release_solver")
+            # memory goes back with the next deferred release
+            self._deferred.append(_Deferred(lambda g=g: _lib.check(g.L.ddhdg_release_solver(g._ctx, 1),
+                                                                  "release_solver")))
             if a.req.bias != 0.0:
                 workloads.set_bias(a.problem, a.req.bias)
                 g.update_boundary_tables()
@@ -356,25 +386,33 @@ class DiodeServer(ThreadedDiodeServer):
                 return False
         return True
 
-    def run(self, requests):
+    def _release_deferred(self):
         import torch
 
+        while self._deferred:
+            self._deferred.pop(0).close()
+        torch.cuda.empty_cache()
+
+    def run(self, requests):
         from .batch import CondenseBatch
 
         reqs = sorted(requests, key=lambda r: r.arrival)
         results, errors = {}, []
         active = []
         committed = 0
-        batches = {}  # (phase, dim) -> (member ids, CondenseBatch)
+        groups = {}  # group key -> {"ids", "batch", "members" of the step in flight or None}
+        self._deferred = []
         self._start_accounting()
         t0 = time.perf_counter()
         i = 0
         while i < len(reqs) or active:
             now = time.perf_counter() - t0
-            # admission at the step boundary
+            # ---- admission
             while i < len(reqs) and reqs[i].arrival <= now and len(active) < self.max_inflight:
                 req = reqs[i]
                 est = memory_estimate(req.dim, req.m, req.k)
+                if not self.admissible(est, committed) and self._deferred:
+                    self._release_deferred()
                 if not self.admissible(est, committed):
                     if not active:
                         errors.append((req.rid, "does not fit in device memory"))
@@ -389,32 +427,51 @@ class DiodeServer(ThreadedDiodeServer):
                 self.peak_inflight = max(self.peak_inflight, len(active))
                 self.peak_committed = max(self.peak_committed, committed)
             if not active:
+                if self._deferred:
+                    self._release_deferred()
                 if i < len(reqs):
                     time.sleep(max(0.0, min(reqs[i].arrival - (time.perf_counter() - t0), 0.05)))
                 continue
-            self.steps += 1
-            done = []
-            # one batch per (phase, dimension): a batched launch holds
-            # devices of one dimension and one mode
-            groups = {}
+            # ---- begin a step in every idle group (rebuilt when its members changed)
+            members_of = {}
             for a in active:
-                groups.setdefault((a.phase, a.req.dim), []).append(a)
-            for bk in sorted(groups):
-                phase, group = bk[0], groups[bk]
-                key = tuple(id(a) for a in group)
-                if bk not in batches or batches[bk][0] != key:
-                    if bk in batches:
-                        batches[bk][1].close()
+                members_of.setdefault(self._group_key(a), []).append(a)
+            for gk, members in members_of.items():
+                gs = groups.get(gk)
+                if gs is not None and gs["members"] is not None:
+                    continue  # its step is running
+                ids = tuple(id(a) for a in members)
+                thermo = gk[0] == "eq"
+                if gs is None or gs["ids"] != ids:
+                    if gs is not None:
+                        self._deferred.append(gs["batch"])
                     bufs = []
-                    for a in group:
-                        if phase not in a.buffers:
-                            a.buffers[phase] = CondenseBatch.buffers_for(a.solver, thermo=(phase == "eq"))
-                        bufs.append(a.buffers[phase])
-                    batches[bk] = (key, CondenseBatch([a.solver for a in group], thermo=(phase == "eq"),
-                                                      buffers=bufs))
-                self.peak_batch = max(self.peak_batch, len(group))
-                norms, status = batches[bk][1].newton_step([a.alpha for a in group])
-                for a, nrm, st in zip(group, norms, status):
+                    for a in members:
+                        if gk[0] not in a.buffers:
+                            a.buffers[gk[0]] = CondenseBatch.buffers_for(a.solver, thermo=thermo)
+                        bufs.append(a.buffers[gk[0]])
+                    gs = groups[gk] = {"ids": ids, "members": None,
+                                       "batch": CondenseBatch([a.solver for a in members], thermo=thermo,
+                                                              buffers=bufs)}
+                gs["batch"].newton_step_begin([a.alpha for a in members])
+                gs["members"] = members
+                self.steps += 1
+                self.peak_batch = max(self.peak_batch, len(members))
+            for gk in [gk for gk, gs in groups.items() if gs["members"] is None and gk not in members_of]:
+                self._deferred.append(groups.pop(gk)["batch"])
+            # ---- collect the steps that have ended
+            done, progressed = [], False
+            for gk, gs in groups.items():
+                if gs["members"] is None:
+                    continue
+                res = gs["batch"].newton_step_end(wait=False)
+                if res is None:
+                    continue
+                progressed = True
+                members, gs["members"] = gs["members"], None
+                phase = gk[0]
+                norms, status = res
+                for a, nrm, st in zip(members, norms, status):
                     a.it += 1
                     upd, cur = max(nrm[0], nrm[1]), max(nrm[2], nrm[3])
                     abs_tol, rel_tol, max_it = a.eq_tol if phase == "eq" else (self.tol, self.tol, self.max_it)
@@ -431,22 +488,25 @@ class DiodeServer(ThreadedDiodeServer):
                 active.remove(a)
                 committed -= a.est
                 g = a.solver
-                torch.cuda.synchronize(self.device)
                 finish = time.perf_counter() - t0
                 state = (g.get_cell_state().copy(), g.get_trace_state().copy()) if self.keep_states else None
                 results[a.req.rid] = Result(a.req.rid, a.req.arrival, a.start, finish, a.total_it, conv,
                                             g.ncells, state)
-                a.solver = None
-                a.buffers = {}
-            if done:
-                # the batches held the finished requests' buffers; hand the
-                # memory back to the device (the trace solver allocates
-                # outside torch's cache)
-                for bk in [bk for bk, (key, _) in batches.items() if any(id(a) in key for a, _ in done)]:
-                    batches.pop(bk)[1].close()
-                torch.cuda.empty_cache()
-        for _, b in batches.values():
-            b.close()
+
+                def drop(a=a):
+                    a.solver = None
+                    a.buffers = {}
+
+                self._deferred.append(_Deferred(drop))
+            if not progressed:
+                if not any(gs["members"] is not None for gs in groups.values()) and self._deferred:
+                    self._release_deferred()
+                time.sleep(0.0005)
+        for gs in groups.values():
+            if gs["members"] is not None:
+                gs["batch"].newton_step_end(wait=True)
+            gs["batch"].close()
+        self._release_deferred()
         if errors:
             raise RuntimeError(f"requests failed: {errors}")
         return [results[r.rid] for r in requests]

@@ -393,6 +393,15 @@ int ddhdg_batch_reconstruct(ddhdg_batch *batch, ddhdg_stream_t stream);
  * step has completed. */
 int ddhdg_batch_newton_step(ddhdg_batch *batch, const double *alpha, double *norms_host,
                             int *status_host, ddhdg_stream_t stream);
+/* The same step in two halves, for a caller that drives several batches
+ * from one host thread: _begin enqueues the step on `stream` and returns at
+ * once (alpha is read before it returns); _end, with wait = 0, returns with
+ * *done = 0 while the step is still running, and otherwise fills
+ * norms_host / status_host as ddhdg_batch_newton_step does and sets
+ * *done = 1.  One step per batch may be in flight. */
+int ddhdg_batch_newton_step_begin(ddhdg_batch *batch, const double *alpha, ddhdg_stream_t stream);
+int ddhdg_batch_newton_step_end(ddhdg_batch *batch, int wait, double *norms_host, int *status_host,
+                                int *done);
 /* Tile shape: cells per tile for degrees 1, 2, 3 (cells_per_tile[3]) and
  * CTAs per SM.  ddhdg_batch_autotune picks them by timing the batch's own
  * condensation launch (coordinate search, best of `reps` launches per

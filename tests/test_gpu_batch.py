@@ -141,3 +141,33 @@ def test_mixed_precision_devices_in_a_batch(dim, sizes, degrees):
     batch.set_shape({1: 4, 2: 8, 3: 1}, 1)
     _check_bitwise(batch, solvers)
     batch.close()
+
+
+def test_newton_step_in_two_halves():
+    """newton_step_begin / newton_step_end give the bits of newton_step, and
+    two batches with steps in flight at the same time do not disturb each
+    other (the serving loop drives its groups this way)."""
+    from ddhdg_b200.batch import CondenseBatch
+
+    specs = workloads.batch_diodes(4, seed=31, sizes=(8, 16), degrees=(1, 2))
+    a_solvers = _solvers(specs, seed=5)
+    b_solvers = _solvers(specs, seed=5)
+    A = CondenseBatch(a_solvers)
+    B = CondenseBatch(b_solvers[:2])
+    C = CondenseBatch(b_solvers[2:])
+    for _ in range(3):
+        nA, sA = A.newton_step([0.5] * 4)
+        B.newton_step_begin([0.5] * 2)
+        C.newton_step_begin([0.5] * 2)
+        rc = None
+        while rc is None:
+            rc = C.newton_step_end(wait=False)
+        nB, sB = B.newton_step_end(wait=True)
+        nC, sC = rc
+        assert sA == sB + sC == [0, 0, 0, 0]
+        assert np.array_equal(nA[:2], nB) and np.array_equal(nA[2:], nC)
+    for g, h in zip(a_solvers, b_solvers):
+        assert np.array_equal(g.get_cell_state(), h.get_cell_state())
+        assert np.array_equal(g.get_trace_state(), h.get_trace_state())
+    for b in (A, B, C):
+        b.close()
