@@ -291,7 +291,11 @@ def run_serve(args):
             "server_steps": server.steps, "peak_batch": server.peak_batch,
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"],
             "solves_per_s": st["solves_per_s"], "cells_per_s": st["cells_per_s"],
-            "converged": st["converged"], "peak_inflight": server.peak_inflight, "wall_s": wall}
+            "converged": st["converged"], "peak_inflight": server.peak_inflight, "wall_s": wall,
+            "per_request": [{"dim": q.dim, "m": q.m, "k": q.k, "bias": round(q.bias, 3),
+                             "arrival_s": round(r.arrival, 3), "wait_s": round(r.start - r.arrival, 3),
+                             "latency_s": round(r.latency, 3), "iterations": r.iterations}
+                            for q, r in zip(reqs, res)]}
     print(json.dumps(line))
 
 

@@ -8,7 +8,7 @@
 // grid of CTAs of BatchTPB threads: every CTA takes the next tile from a
 // counter, loads that device's launch parameters into shared memory and runs
 // the per-degree body on the tile's cells (the unit-cell constant tables of
-// every degree travel in the constant bank): four warps on four cells at a time
+// every degree travel in the constant bank): two warps on two cells at a time
 // for the warp-per-cell degrees (condense3_cells, FP64 or with the FP32
 // Jacobian of a mixed-precision device), the whole CTA on one cell at a time
 // otherwise (condense2_cells).  Tiles are ordered heaviest first; their sizes
@@ -27,7 +27,7 @@
 
 namespace ddhdg
 {
-  constexpr int BatchTPB  = CondenseTPB; // 128: 4 warps
+  constexpr int BatchTPB  = 64;          // 2 warps: two cells at a time, or one CTA-per-cell cell
   constexpr int BatchWarp = BatchTPB / 32;
   constexpr int BatchRTPB = 256;         // reconstruction: 8 warps
 
@@ -106,16 +106,17 @@ namespace ddhdg
                                     t.end, BatchWarp);
       }
     else if constexpr (sizeof(JT) == 8)
-      condense2_cells<DIM, K>(P, smem, blockIdx.x, t.begin, t.end, 1);
+      condense2_cells<DIM, K, BatchTPB>(P, smem, blockIdx.x, t.begin, t.end, 1);
   }
 
   // The precisions a batch holds: FP64 devices only, mixed-precision
   // warp-per-cell devices only, or both.  Each class is its own
   // instantiation, so that a batch carries only the bodies it runs: the
-  // mixed-only kernel is built for four CTAs per SM (128 registers), the
-  // occupancy of the single-device mixed kernel; the others for two (the
-  // FP64 bodies take 255 registers, and the mixed bodies beside them add
-  // spills).
+  // mixed-only kernel is built for eight CTAs of two warps per SM (128
+  // registers), the occupancy of the single-device mixed kernel; the others
+  // for four (the FP64 bodies take 255 registers, and the mixed bodies
+  // beside them add spills).  Small CTAs keep several CTA-per-cell cells
+  // on an SM, so that their serial LU panels overlap.
   enum BatchPrec : int
   {
     BatchFP64  = 0,
@@ -125,7 +126,7 @@ namespace ddhdg
 
   // counter: tiles handed out so far (zero at launch)
   template <int DIM, int PREC>
-  __global__ void __launch_bounds__(BatchTPB, PREC == BatchMixed ? 4 : 2)
+  __global__ void __launch_bounds__(BatchTPB, PREC == BatchMixed ? 8 : 4)
   batch_condense_kernel(const BatchJob *__restrict__ jobs, const BatchTile *__restrict__ tiles,
                         int ntiles, int *counter, const __grid_constant__ BatchTabs<DIM> C)
   {

@@ -1361,7 +1361,6 @@ ddhdg_release_solver(ddhdg_ctx *c, int thermo)
 {
   if (!c)
     return fail(DDHDG_BAD_ARG, "null argument");
-  CK(cudaDeviceSynchronize()); // no solve of this context may be in flight
   c->mode[thermo ? 1 : 0].nd.reset();
   return DDHDG_OK;
 }
@@ -2227,7 +2226,7 @@ struct ddhdg_batch
   DevBuf<int>              counter; // [0]: condense, [1]: reconstruct
   bool                     degrees[4]        = {false, false, false, false};
   int                      cells_per_tile[4] = {0, 32, 32, 4};
-  int                      ctas_per_sm       = 4; // at most; the kernel's occupancy limit applies
+  int                      ctas_per_sm       = 8; // at most; the kernel's occupancy limit applies
   int                      occ_c             = 0; // CTAs per SM the condense kernel allows
   int                      rcells_per_tile   = 256;
   int                      ntiles_c = 0, ntiles_r = 0, grid_c = 0, grid_r = 0;
@@ -2884,9 +2883,9 @@ ddhdg_batch_autotune(ddhdg_batch *b, int reps, float *best_ms, ddhdg_stream_t st
         }
     }
   // CTAs per SM: 1 up to what the kernel's registers and the batch's
-  // shared memory allow (at most 4)
+  // shared memory allow (at most 8)
   b->ctas_per_sm = std::min(b->ctas_per_sm, b->occ_c);
-  for (int cps = 1; cps <= std::min(4, b->occ_c); ++cps)
+  for (int cps = 1; cps <= std::min(8, b->occ_c); ++cps)
     {
       if (cps == b->ctas_per_sm)
         continue;

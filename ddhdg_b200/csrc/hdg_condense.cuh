@@ -378,11 +378,12 @@ namespace ddhdg
       }
   }
 
-  // The body of the CTA-per-cell condensation: the CTA (CondenseTPB threads)
-  // works through the cells cell_begin, cell_begin + cell_step, ... <
-  // cell_end with the workspace at smem (tables first when P.stage) and, for
-  // R outside shared memory, the R slice `slot` of P.rscratch.
-  template <int DIM, int K>
+  // The body of the CTA-per-cell condensation: the CTA (T threads, a
+  // multiple of 32: CondenseTPB in condense2_kernel, fewer in the batched
+  // launch) works through the cells cell_begin, cell_begin + cell_step, ...
+  // < cell_end with the workspace at smem (tables first when P.stage) and,
+  // for R outside shared memory, the R slice `slot` of P.rscratch.
+  template <int DIM, int K, int T = CondenseTPB>
   __device__ __forceinline__ void
   condense2_cells(const KParams &P, double *smem, int64_t slot, int64_t cell_begin,
                   int64_t cell_end, int64_t cell_step)
@@ -396,7 +397,6 @@ namespace ddhdg
     constexpr int Fq  = F * nqf;
     constexpr int Ft  = F * nf;
     constexpr int NCA = Dm::Nc_all;
-    constexpr int T   = CondenseTPB;
     constexpr int NW  = T / 32;
     __shared__ int sh_p8[CtaLuNB];
     __shared__ int sh_sing;

@@ -136,7 +136,7 @@ def request_precision(req: Request, mixed: bool) -> int:
 
 def solve_one(req: Request, device="cuda:0", keep_state=False, tol=1e-10, max_it=50, mixed=False):
     """One request's solve on the calling thread's current CUDA stream."""
-    from . import _lib, workloads
+    from . import workloads
     from .solver import NPSolver
 
     pb, prm, adim = workloads.diode(dim=req.dim, m=req.m, k=req.k, precision=request_precision(req, mixed))
@@ -145,8 +145,6 @@ def solve_one(req: Request, device="cuda:0", keep_state=False, tol=1e-10, max_it
     g = NPSolver(pb, prm, adim, device=device)
     res = g.compute_thermodynamic_equilibrium()
     it = res.iterations
-    # the equilibrium system's trace solver is not used again
-    _lib.check(g.L.ddhdg_release_solver(g._ctx, 1), "release_solver")
     if req.bias != 0.0:
         workloads.set_bias(pb, req.bias)
         g.update_boundary_tables()

@@ -254,8 +254,9 @@ int ddhdg_set_solver_graphs(ddhdg_ctx *ctx, int enable);
  * (thermo_eq 0: the full system, 1: the equilibrium system): its fronts,
  * library handles, side streams and graphs.  The next solve of that mode
  * builds it again (the host plan comes from the process-wide cache).  A
- * serving loop calls it when a request leaves the equilibrium phase.
- * Synchronises the device first. */
+ * serving loop calls it when a request leaves the equilibrium phase.  No
+ * solve of that mode may be in flight (the caller's to ensure); freeing
+ * device memory waits for the device. */
 int ddhdg_release_solver(ddhdg_ctx *ctx, int thermo_eq);
 
 /* No counterpart in the reference (its solve is UMFPACK or GMRES on the
