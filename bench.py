@@ -321,6 +321,56 @@ def serve_quick(n=10, rate=4.0, seed=7):
                         "bias U[0, 0.8] V, mixed-precision condensation (full-size stream: bench.py --serve)"}
 
 
+def batch_quick(n=64, steps=5):
+    """The first n diodes of the batched configuration (seed 2025: mesh
+    cells per side U[16, 128], degree U{1, 2, 3}) condensed in one launch and
+    reconstructed in one more per step, tile shapes autotuned: cells/s for
+    the default bench line (the full 512-diode batch: bench.py --batch)."""
+    import torch
+
+    from ddhdg_b200 import _lib
+    from ddhdg_b200 import workloads as cases
+    from ddhdg_b200.batch import CondenseBatch
+    from ddhdg_b200.solver import NPSolver
+
+    specs = cases.batch_diodes(512, seed=2025)[:n]
+    solvers = []
+    for pb, prm, adim, _ in specs:
+        g = NPSolver(pb, prm, adim)
+        g.compute_local_charge_neutrality()
+        for c in (1, 2):
+            _lib.check(g.L.ddhdg_project_density(g._ctx, c, 0.0, g.cell_state.data_ptr(),
+                                                 g.trace_state.data_ptr(), g._sp()), "project_density")
+        solvers.append(g)
+    batch = CondenseBatch(solvers)
+    for i in range(n):
+        batch.update_trace[i].fill_(1e-6)
+    batch.autotune(reps=1)
+    stream = batch.stream
+    for _ in range(3):
+        batch.condense()
+        batch.reconstruct()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    for _ in range(steps):
+        batch.condense()
+    ev[1].record(stream)
+    for _ in range(steps):
+        batch.reconstruct()
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    cm, rm = ev[0].elapsed_time(ev[1]) / steps, ev[1].elapsed_time(ev[2]) / steps
+    out = {"devices": n, "cells": batch.cells, "condense_ms": cm, "reconstruct_ms": rm,
+           "cells_per_s": batch.cells / ((cm + rm) * 1e-3), "launches_per_step": 2, "shape": batch.shape(),
+           "workload": "the first 64 diodes of the 512-diode batch (seed 2025; 2D, cells per side U[16,128], "
+                       "degree U{1,2,3}), FP64 (full batch: bench.py --batch)"}
+    batch.close()
+    del solvers
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_bias_sweep(args):
     """The second diode configuration end to end: equilibrium, then a forward
     bias sweep 0.0..0.8 V in 0.05 V steps, each point warm-started, every
@@ -625,7 +675,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-serve", action="store_true", help="skip the short serving stream of the default line")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="skip the short serving stream and the 64-diode batch of the default line")
     ap.add_argument("--serve", action="store_true",
                     help="serve a seeded Poisson stream of diode solves and report p50/p99 latency")
     ap.add_argument("--serve-requests", type=int, default=24)
@@ -945,6 +996,7 @@ def main():
     serve = None
     if world == 1 and not args.no_serve:
         serve = serve_quick()
+    batchq = batch_quick() if world == 1 and not args.no_serve else None
 
     fp64_peak = fp64_peak_tflops(dev)
     if rank == 0:
@@ -984,6 +1036,7 @@ def main():
             "plain": plain,
             "target": target,
             "serve": serve,
+            "batch": batchq,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }
