@@ -838,9 +838,8 @@ namespace ddhdg
         // high word of |S'_ij| (sign, exponent and 20 mantissa bits) with the
         // low 5 bits replaced by 31 - lane: the pivot is within 2^-15 of the
         // largest candidate, ties go to the lowest lane.  The pivot row is
-        // broadcast through shared memory (the coefficient block, dead here).
+        // broadcast by shuffles, element by element as the update uses it.
         static_assert(NSMAX < 32, "key 0 marks used lanes");
-        JT     *prow  = reinterpret_cast<JT *>(coef);
         bool    used  = lane >= NSMAX;
         int     mypos = 0;
         bool    sing  = false;
@@ -856,21 +855,14 @@ namespace ddhdg
             const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
             const int      bl   = 31 - (int)(kmax & 31u);
             const bool     me   = lane == bl;
-            if (me)
-              {
-#pragma unroll
-                for (int k = 0; k < NSMAX; k += 2)
-                  store_pair(prow + k, srow[k], k + 1 < NSMAX ? srow[k + 1] : JT(0));
-              }
-            __syncwarp();
-            const JT pj = prow[0];
+            const JT pj = __shfl_sync(0xffffffffu, srow[0], bl);
             sing |= kmax < 32u || !isfinite(pj);
             const JT hr = (pj != JT(0)) ? JT(1) / pj : JT(0);
             const JT l  = srow[0] * hr;
 #pragma unroll
             for (int k = 1; k < NSMAX; ++k)
               {
-                const JT pk = prow[k];
+                const JT pk = __shfl_sync(0xffffffffu, srow[k], bl);
                 srow[k - 1]     = me ? -pk * hr : srow[k] - l * pk;
               }
             srow[NSMAX - 1] = me ? hr : l;
