@@ -3,12 +3,14 @@
 Requests (a diode's dimension, mesh, degree and bias) arrive over time.  The
 server admits a request as soon as an in-flight slot and enough free device
 memory are available, and keeps its Newton state on the device for the whole
-solve.  ``DiodeServer`` batches at kernel level, step by step: every request
-in flight advances one Newton step per server step, the assembly and
-condensation of all requests in the same phase run as ONE batched launch
-(``ddhdg_batch_newton_step``), their trace solves overlap on side streams,
-and the reconstruction is one more launch; requests join at the next step
-after they arrive and leave when they converge (continuous batching).
+solve.  ``DiodeServer`` batches at kernel level: the requests in flight form
+groups by (phase, dimension, size class), and a group advances all its
+requests by one Newton step at a time, their assembly and condensation as
+ONE batched launch (``ddhdg_batch_newton_step_begin``), their trace solves
+overlapped on side streams, and the reconstruction as one more launch.
+Groups step independently on their own streams, so small requests are not
+held back by large ones; requests join their group at its next step after
+they arrive and leave when they converge (continuous batching).
 ``ThreadedDiodeServer`` is the simpler form: one host thread, context and
 stream per request, overlapping only on the device.  Results do not depend on
 what else runs: every kernel is deterministic (no atomics with more than two
@@ -85,9 +87,9 @@ def memory_estimate(dim: int, m: int, k: int) -> int:
     """Device bytes of one solve: the trace solvers of both phases (the
     V-only equilibrium system's is released only when no step is in flight,
     so it may still be held while the biased system's is built) from their
-    plans, the global trace sparsity,
-    the per-cell states, condensed blocks and Y cache of both phases, and the
-    per-request overhead; the array terms 10 % over."""
+    plans, the global trace sparsity, the per-cell states, condensed blocks
+    and Y caches of both phases, and the per-request overhead; the array
+    terms 10 % over."""
     nb = (k + 1) ** dim
     nf = (k + 1) ** (dim - 1)
     cells = m ** dim
