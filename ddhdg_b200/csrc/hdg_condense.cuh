@@ -104,15 +104,17 @@ namespace ddhdg
   // row stride ncol), then U Y = R' by block back substitution; R becomes Y.
   // Right-looking, panels of CtaLuNB columns:
   // - warp 0 factorises the panel with its rows in registers (pivot search
-  //   by a warp reduction over the rows below the diagonal, the pivot row
-  //   exchanged and broadcast by shuffles, multipliers inside the panel);
+  //   by one redux of a packed key over the rows below the diagonal, as in
+  //   the warp-per-cell Gauss-Jordan; the pivot row exchanged and broadcast
+  //   by shuffles; multipliers inside the panel);
   // - the CTA, a thread per column, applies the panel's row swaps to the
   //   columns right of it (S, then R) and solves the panel rows of U there
   //   with the unit lower panel block;
   // - the trailing update A22 -= L21 U12 runs on the FP64 tensor path in
   //   8 x 8 tiles (K = the panel width), the warps taking tiles in turn.
-  // The pivots are those of the unblocked factorisation: each panel sees its
-  // columns fully updated.  The multipliers of finished panels are not
+  // Each panel sees its columns fully updated, so the pivots are those of
+  // the unblocked factorisation up to the key's rounding (2^-13).  The
+  // multipliers of finished panels are not
   // swapped (nothing reads them again).  Back substitution per panel block
   // from the bottom: the diagonal block a thread per column of R, then the
   // rows above on the tensor path.  Three barriers per panel and two per
@@ -162,25 +164,18 @@ namespace ddhdg
                         bi   = row;
                       }
                   }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1)
-                  {
-                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                    const int    oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                    if (ob > best || (ob == best && oi < bi))
-                      {
-                        best = ob;
-                        bi   = oi;
-                      }
-                  }
-                if (bi >= Ns)
-                  bi = j; // no finite candidate: keep the row (singular)
+                // one warp max-reduction of a 32-bit key: the high word of
+                // |candidate| with the low 7 bits replaced by 127 - its row
+                // offset in the panel (the pivot is within 2^-13 of the
+                // largest candidate, ties go to the lowest row)
+                unsigned key = 0u;
+                if (bi < Ns)
+                  key = ((unsigned)((unsigned long long)__double_as_longlong(best) >> 32) & ~127u) |
+                        (127u - (unsigned)(bi - j0));
+                const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+                bi = kmax ? j0 + 127 - (int)(kmax & 127u) : j; // none: keep the row (singular)
                 if (lane == 0)
-                  {
-                    sh_p[jj] = bi;
-                    if (!(best > 0.) || !isfinite(best))
-                      sh_sing = 1;
-                  }
+                  sh_p[jj] = bi;
                 const int oj = (j - j0) & 31, sj = (j - j0) >> 5;
                 if (bi != j)
                   {
@@ -219,6 +214,8 @@ namespace ddhdg
                   }
                 const double d   = prow[jj];
                 const double inv = (d != 0.) ? 1. / d : 0.;
+                if (lane == 0 && (!(fabs(d) > 0.) || !isfinite(d)))
+                  sh_sing = 1;
 #pragma unroll
                 for (int r = 0; r < PR; ++r)
                   {
