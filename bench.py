@@ -968,7 +968,7 @@ def main():
     del gn
     torch.cuda.empty_cache()
 
-    # ---- the north-star comparison: condensation per Newton step of the
+    # ---- the target comparison: condensation per Newton step of the
     # mixed-precision and FP64 block-eliminated paths against the plain FP64
     # GPU path, and the whole Newton step (the trace solve is the same in all)
     fp64_c = float(np.mean(cond_ms))
