@@ -1013,7 +1013,8 @@ def main():
             "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"2D p-n diode {m_side}x{m_side} quads (cell size 1/256 um), HDG degree 2, FP64, plain method",
+            "config": {"workload": f"2D p-n diode {m_side}x{m_side} quads (cell size 1/256 um), HDG degree 2, FP64, "
+                                   "block-eliminated condensation (the plain FP64 path is the `plain` key)",
                        "cells": nc, "trace_dofs_per_cell": Nt,
                        "parallelism": f"replicas x{world}",
                        "l2": "per-step traffic (>1.2 GB) exceeds the 126 MB L2"},
