@@ -208,7 +208,7 @@ namespace ddhdg
   template <int DIM, int K, typename JT>
   __device__ __forceinline__ void
   condense3_cells(const KParams &P, const CTab<DIM, K> &C, double *ws, int *piv,
-                  int64_t cell_begin, int64_t cell_end, int64_t cell_step)
+                  int64_t cell_begin, int64_t cell_end, int64_t cell_step, const double *rqr = nullptr)
   {
     using Dm            = Dims<DIM, K>;
     constexpr int nb    = Dm::nb;
@@ -240,7 +240,10 @@ namespace ddhdg
     const double *TLg    = tb + P.to.TLg;
     const double *TLf    = tb + P.to.TLf;
     const double *RTr    = tb + P.to.RTr;
-    const double *RQr    = tb + P.to.RQr;
+    // the face-flux table of the trace rows, read at lane-dependent
+    // addresses in the tt epilogue: a per-CTA copy in shared memory when
+    // the caller staged one (the same values as the table's)
+    const double *RQr    = rqr ? rqr : tb + P.to.RQr;
     const double *PW_c   = tb + P.to.PW_c;
     const double *PW_f   = tb + P.to.PW_f;
     const double *QW_c   = tb + P.to.QW_c;
@@ -1170,12 +1173,16 @@ namespace ddhdg
   condense3_kernel(const KParams P, const __grid_constant__ CTab<DIM, K> C)
   {
     extern __shared__ __align__(16) double smem[];
-    __shared__ int piv3[Condense3MaxWPB][3 * Dims<DIM, K>::nb];
+    __shared__ int    piv3[Condense3MaxWPB][3 * Dims<DIM, K>::nb];
+    __shared__ double rqr_s[CTab<DIM, K>::Fq * CTab<DIM, K>::Ft];
+    for (int i = threadIdx.x; i < CTab<DIM, K>::Fq * CTab<DIM, K>::Ft; i += blockDim.x)
+      rqr_s[i] = P.tables[P.to.RQr + i];
+    __syncthreads();
     const int      warp = threadIdx.x >> 5;
     const int      wpb  = blockDim.x >> 5;
     const Ws3Off   wo   = ws3_layout(DIM, Dims<DIM, K>::nb, Dims<DIM, K>::nf, P.ncomp, P.ncol, (int)sizeof(JT));
     condense3_cells<DIM, K, JT>(P, C, smem + warp * wo.total, piv3[warp],
                                 P.cell0 + (int64_t)blockIdx.x * wpb + warp, P.ncells,
-                                (int64_t)gridDim.x * wpb);
+                                (int64_t)gridDim.x * wpb, rqr_s);
   }
 } // namespace ddhdg
