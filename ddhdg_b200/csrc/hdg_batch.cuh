@@ -102,8 +102,15 @@ namespace ddhdg
       {
         const int    warp = threadIdx.x >> 5;
         const Ws3Off wo   = ws3_layout(DIM, Dims<DIM, K>::nb, Dims<DIM, K>::nf, P.ncomp, P.ncol, (int)sizeof(JT));
+        // the device's face-flux table of the tt epilogue, after the warps'
+        // workspaces (as the single-device kernel stages it)
+        constexpr int NR  = CTab<DIM, K>::Fq * CTab<DIM, K>::Ft;
+        double       *rqr = smem + BatchWarp * wo.total;
+        for (int i = threadIdx.x; i < NR; i += BatchTPB)
+          rqr[i] = P.tables[P.to.RQr + i];
+        __syncthreads();
         condense3_cells<DIM, K, JT>(P, batch_tab<K>(C), smem + warp * wo.total, piv[warp], t.begin + warp,
-                                    t.end, BatchWarp);
+                                    t.end, BatchWarp, rqr);
       }
     else if constexpr (sizeof(JT) == 8)
       condense2_cells<DIM, K, BatchTPB>(P, smem, blockIdx.x, t.begin, t.end, 1);

@@ -2571,7 +2571,9 @@ ddhdg_batch_create(const ddhdg_batch_item *items, int n, int thermo, ddhdg_batch
       if (3 * c->nb <= 32)
         {
           const Ws3Off w = ws3_layout(c->dim, c->nb, c->nf, m.ncomp, m.ncol, J.mixed ? 4 : 8);
-          b->smem_c      = std::max(b->smem_c, (size_t)BatchWarp * w.total * sizeof(double));
+          // the warps' workspaces and the staged face-flux table
+          b->smem_c = std::max(b->smem_c, ((size_t)BatchWarp * w.total +
+                                           (size_t)(c->F * c->nqf) * (c->F * c->nf)) * sizeof(double));
           J.P.wpb        = 1;
           J.P.stage      = 0;
         }
